@@ -1,0 +1,76 @@
+"""Pins the oracle to the reference: the 8 testsets of test/runtests.jl, with the
+reference's own grids, models and tolerances, run against the C++ restatement.
+
+The tolerances in the reference tests are its observed errors rounded up at the last
+digit, so passing them is a tight check of the restatement.
+"""
+import numpy as np
+import pytest
+
+import eikoracle as O
+import refcases as RC
+
+# The reference's FD tolerances are its observed adjoint-vs-FD errors rounded up at the
+# 3rd digit. Central differences of a misfit of size M with step dh carry rounding noise
+# of order eps*M/(2*dh) (1e-8..3e-6 absolute for these cases, up to ~1% of the error),
+# and Julia's SIMD `sum` rounds differently from any C/numpy sum. FD_SLACK absorbs that
+# noise; FD_FLOOR checks that the error is the reference's error, not a smaller one.
+FD_SLACK = 1.015
+FD_FLOOR = 0.90
+
+
+@pytest.mark.parametrize("case", RC.all_forward_cases(), ids=lambda c: c["name"])
+def test_forward_vs_analytic(case):
+    _, tt = O.eiktraveltime(case["vel"], case["grd"], case["coordsrc"], case["coordrec"],
+                            returntt=True, extraparams=case["extraparams"])
+    d = tt[0] - case["analytic"]
+    maxerr, normerr = np.abs(d).max(), np.linalg.norm(d)
+    assert maxerr <= case["tolerr"] and normerr <= case["tolnorm"], (maxerr, normerr)
+    # the tolerances are the reference's observed errors rounded up: we should be close
+    assert maxerr >= 0.5 * case.get("observed", case["tolerr"])
+
+
+def _misfit_fn(c):
+    grd, rec, ep = c["grd"], c["coordrec"], c["extraparams"]
+
+    def obs():
+        picks = O.eiktraveltime(c["velmod"], grd, c["coordsrc1"], rec, extraparams=ep)
+        std = [0.0001 * np.ones(p.shape) for p in picks]
+        return picks, std
+    return obs
+
+
+@pytest.mark.parametrize("case", RC.gradvel_2D() + RC.gradvel_3D(), ids=lambda c: c["name"])
+def test_gradvel_vs_fd(case):
+    grd, rec, ep = case["grd"], case["coordrec"], case["extraparams"]
+    dobs, stdobs = _misfit_fn(case)()
+    gv, misf1 = O.eikgradient(case["vel0"], grd, case["coordsrc2"], rec, dobs, stdobs, "gradvel",
+                              extraparams=ep)
+    misf2 = O.eikttimemisfit(case["vel0"], grd, case["coordsrc2"], rec, dobs, stdobs, extraparams=ep)
+    assert np.isclose(misf1, misf2, rtol=1.4901161193847656e-8, atol=0)
+
+    def picks(v):
+        return O.eiktraveltime(v, grd, case["coordsrc2"], rec, extraparams=ep)
+    fd = RC.fd_gradvel(picks, case["vel0"], case["dh"], dobs, stdobs)
+    d = np.abs(gv - fd)
+    mx, nrm = d.max(), np.linalg.norm(d)
+    assert mx <= FD_SLACK * case["tolerr"] and nrm <= FD_SLACK * case["tolnorm"], (mx, nrm)
+    assert mx >= FD_FLOOR * case["tolerr"] and nrm >= FD_FLOOR * case["tolnorm"], (mx, nrm)
+
+
+@pytest.mark.parametrize("case", RC.gradsrc_2D() + RC.gradsrc_3D(), ids=lambda c: c["name"])
+def test_gradsrcloc_vs_fd(case):
+    grd, rec, ep = case["grd"], case["coordrec"], case["extraparams"]
+    dobs, stdobs = _misfit_fn(case)()
+    gs, misf1 = O.eikgradient(case["vel0"], grd, case["coordsrc2"], rec, dobs, stdobs, "gradsrcloc",
+                              extraparams=ep)
+    misf2 = O.eikttimemisfit(case["vel0"], grd, case["coordsrc2"], rec, dobs, stdobs, extraparams=ep)
+    assert np.isclose(misf1, misf2, rtol=1.4901161193847656e-8, atol=0)
+
+    def picks_src(cs):
+        return O.eiktraveltime(case["vel0"], grd, cs, rec, extraparams=ep)
+    fd = RC.fd_gradsrc(picks_src, case["coordsrc2"], case["dh"], dobs, stdobs)
+    d = np.abs(gs - fd)
+    mx, nrm = d.max(), np.linalg.norm(d)
+    assert mx <= FD_SLACK * case["tolerr"] and nrm <= FD_SLACK * case["tolnorm"], (gs, fd)
+    assert mx >= FD_FLOOR * case["tolerr"] and nrm >= FD_FLOOR * case["tolnorm"], (gs, fd)
