@@ -1,0 +1,271 @@
+// Local 2nd-order upwind update of EikonalSolvers.jl (calcttpt_2ndord!,
+// src/EikSolv/eikforward2D.jl:98-433 and src/EikSolv/eikforward3D.jl:151-532) and the
+// order rule that turns it into a fixed-point problem solvable in parallel.
+//
+// The reference evaluates the update inside a heap-ordered fast-marching loop
+// (ttFMM_core!, src/EikSolv/eikmainfwd.jl:427-823): a node is recomputed each time one
+// of its 2*nd immediate neighbours is accepted, using only accepted nodes, and keeps the
+// value of its last recomputation. This header restates that final value as a function
+// of the neighbourhood alone ("prefix rule"):
+//
+//   sort the immediate neighbours by acceptance key (source points first, then
+//   traveltime); for each group g of equal keys K_g, evaluate the update with
+//   accepted(x) := key(x) <= K_g; the first group whose result v_g does not exceed the
+//   key of the next group is the one after which the node is accepted itself, so v_g is
+//   its traveltime and the derivative codes of that evaluation are its codes.
+//
+// Iterating the rule on every node from t = +inf to a fixed point reproduces the FMM
+// traveltimes bit for bit: keys (below) place the rare non-causal acceptances of the
+// reference (an overwritten band value below the current front) right after the node
+// that triggered them, as the heap does.
+//
+// The arithmetic is the reference's, operation by operation (x^2 as x*x, left-to-right
+// sums, no FMA contraction: translation units including this header are compiled with
+// --fmad=false / -ffp-contract=off).
+#pragma once
+
+#include <cstdint>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define EIK_HD __host__ __device__ __forceinline__
+#else
+#define EIK_HD inline
+#endif
+
+namespace eik {
+
+#ifndef EIK_INF
+#define EIK_INF (__builtin_huge_val())
+#endif
+
+// Acceptance key: the position at which the heap-ordered FMM accepts a node, as a
+// lexicographic triple (L, d, t). A node accepted in the batch of its own traveltime t has
+// key (t, 0, t). A node whose last recomputation, triggered by the acceptance of a node of
+// key (L, d, .), produced a value v <= L is accepted right after that trigger although v is
+// below the current front (the reference overwrites band values, BinHeaps.jl:394-430, and
+// takes no causality check, eikforward2D.jl:425-430): its key is (L, d+1, v). Source points
+// are accepted together before anything else: key (-inf, 0, -inf).
+#ifndef EIK_MAX_DEPTH
+#define EIK_MAX_DEPTH 4
+#endif
+struct Key {
+  double L;
+  int d;
+  double t;
+};
+EIK_HD bool key_le(const Key& a, const Key& b) {
+  if (a.L != b.L) return a.L < b.L;
+  if (a.d != b.d) return a.d < b.d;
+  return a.t <= b.t;
+}
+EIK_HD bool key_eq(const Key& a, const Key& b) { return a.L == b.L && a.d == b.d && a.t == b.t; }
+EIK_HD Key key_normal(double t) { return Key{t, 0, t}; }
+EIK_HD Key key_source() { return Key{-EIK_INF, 0, -EIK_INF}; }
+EIK_HD Key key_unreached() { return Key{EIK_INF, 0, EIK_INF}; }
+EIK_HD bool key_reached(const Key& k) { return k.L < EIK_INF; }
+
+// Neighbourhood of one node as seen by the update. Index [axis][side]: side 0 is the
+// +1 neighbour (l=1 in the reference), side 1 the -1 neighbour (l=2).
+struct Nbhd {
+  double t1[3][2];   // traveltime at distance 1 (+inf if not reached / outside)
+  double t2[3][2];   // traveltime at distance 2
+  Key k1[3][2];      // acceptance key at distance 1
+  Key k2[3][2];      // acceptance key at distance 2
+  bool in1[3][2];    // !isonb1: distance-1 node inside the grid
+  bool ok2[3][2];    // !isonb2 of the distance-1 node (2nd order allowed on that side)
+  double dh[3];      // node spacing per axis
+  double slow;       // 1/vel at the node (computed as 1.0/vel, as the reference)
+};
+
+// calcttpt_2ndord! with accepted(x) := key(x) <= T. codes receive the reference's
+// derivative codes (codeD): -side for 1st order, -2*side for 2nd order, 0 unused.
+template <int ND>
+EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdisc) {
+  double alpha = 0.0, beta = 0.0, gamma = -(nb.slow * nb.slow);
+#pragma unroll
+  for (int a = 0; a < ND; a++) codes[a] = 0;
+#pragma unroll
+  for (int a = 0; a < ND; a++) {
+    bool use1 = false, use2 = false;
+    double cv1 = EIK_INF, cv2 = EIK_INF;
+#pragma unroll
+    for (int l = 0; l < 2; l++) {
+      const int sh = l == 0 ? 1 : -1;
+      if (nb.in1[a][l] && key_le(nb.k1[a][l], T)) {
+        const double tv1 = nb.t1[a][l];
+        if (tv1 < cv1) {
+          cv1 = tv1;
+          use1 = true;
+          codes[a] = (int8_t)(-sh);
+          if (nb.ok2[a][l] && key_le(nb.k2[a][l], T)) {
+            const double tv2 = nb.t2[a][l];
+            if (tv2 <= cv1) {
+              cv2 = tv2;
+              use2 = true;
+              codes[a] = (int8_t)(-2 * sh);
+            } else {
+              cv2 = EIK_INF;
+              use2 = false;
+              codes[a] = (int8_t)(-sh);
+            }
+          }
+        }
+      }
+    }
+    const double dh = nb.dh[a];
+    if (use2 && use1) {
+      const double tmpa2 = (1.0 / 3.0) * (4.0 * cv1 - cv2);
+      const double ca = 9.0 / (4.0 * (dh * dh));
+      alpha += ca;
+      beta += (-2.0 * ca) * tmpa2;
+      gamma += ca * (tmpa2 * tmpa2);
+    } else if (use1) {
+      const double ca = 1.0 / (dh * dh);
+      alpha += ca;
+      beta += (-2.0 * ca) * cv1;
+      gamma += ca * (cv1 * cv1);
+    }
+  }
+  double sqarg = beta * beta - (4.0 * alpha) * gamma;
+  if (sqarg < 0.0) {  // 1st order on every axis (eikforward2D.jl:265-337)
+    alpha = 0.0;
+    beta = 0.0;
+    gamma = -(nb.slow * nb.slow);
+#pragma unroll
+    for (int a = 0; a < ND; a++) {
+      codes[a] = 0;
+      bool use1 = false;
+      double cv1 = EIK_INF;
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        const int sh = l == 0 ? 1 : -1;
+        if (nb.in1[a][l] && key_le(nb.k1[a][l], T)) {
+          const double tv1 = nb.t1[a][l];
+          if (tv1 < cv1) {
+            cv1 = tv1;
+            use1 = true;
+            codes[a] = (int8_t)(-sh);
+          }
+        }
+      }
+      if (use1) {
+        const double dh = nb.dh[a];
+        const double ca = 1.0 / (dh * dh);
+        alpha += ca;
+        beta += (-2.0 * ca) * cv1;
+        gamma += ca * (cv1 * cv1);
+      }
+    }
+    sqarg = beta * beta - (4.0 * alpha) * gamma;
+  }
+  if (sqarg < 0.0) {  // one-dimensional update (eikforward2D.jl:340-411)
+    if (negdisc) *negdisc = true;
+    double cv[3] = {EIK_INF, EIK_INF, EIK_INF};
+    int8_t cd[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < ND; a++) {
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        const int sh = l == 0 ? 1 : -1;
+        if (nb.in1[a][l] && key_le(nb.k1[a][l], T)) {
+          const double tv1 = nb.t1[a][l];
+          if (tv1 < cv[a]) {
+            cv[a] = tv1;
+            cd[a] = (int8_t)(-sh);
+          }
+        }
+      }
+    }
+    int id = 0;
+#pragma unroll
+    for (int a = 1; a < ND; a++)
+      if (cv[a] < cv[id]) id = a;
+#pragma unroll
+    for (int a = 0; a < ND; a++) codes[a] = (a == id) ? cd[a] : (int8_t)0;
+    return (nb.dh[id] * nb.slow) + cv[id];
+  }
+  const double tmpsq = sqrt(sqarg);
+  const double s1 = (-beta + tmpsq) / (2.0 * alpha);
+  const double s2 = (-beta - tmpsq) / (2.0 * alpha);
+  return (s2 > s1) ? s2 : s1;
+}
+
+// Prefix rule: returns the node's traveltime (+inf if no neighbour is reached yet),
+// writes its derivative codes and its own acceptance key.
+template <int ND>
+EIK_HD double prefix_rule(const Nbhd& nb, int8_t* codes, Key* key_out, bool* negdisc) {
+  // distinct keys of the reached in-grid immediate neighbours, ascending
+  Key keys[2 * ND];
+  int nk = 0;
+#pragma unroll
+  for (int a = 0; a < ND; a++)
+#pragma unroll
+    for (int l = 0; l < 2; l++) {
+      const Key k = nb.k1[a][l];
+      if (nb.in1[a][l] && key_reached(k)) {
+        bool dup = false;
+        for (int q = 0; q < nk; q++)
+          if (key_eq(keys[q], k)) dup = true;
+        if (!dup) {
+          int p = nk;
+          while (p > 0 && !key_le(keys[p - 1], k)) {
+            keys[p] = keys[p - 1];
+            p--;
+          }
+          keys[p] = k;
+          nk++;
+        }
+      }
+    }
+#pragma unroll
+  for (int a = 0; a < ND; a++) codes[a] = 0;
+  double vprev = EIK_INF;
+  Key kprev = key_unreached();
+  int8_t cprev[3] = {0, 0, 0};
+  for (int g = 0; g < nk; g++) {
+    int8_t cg[3];
+    const double v = update_at<ND>(nb, keys[g], cg, negdisc);
+    const Key& kg = keys[g];
+    if (!(v > kg.L) && kg.d >= EIK_MAX_DEPTH && g > 0) {
+      // A cascade of non-causal acceptances deeper than the heap ever produces: the
+      // group is ordered after this node (transient of the iteration, not an FMM state).
+#pragma unroll
+      for (int a = 0; a < ND; a++) codes[a] = cprev[a];
+      *key_out = kprev;
+      return vprev;
+    }
+    const Key mine = (v > kg.L) ? key_normal(v) : Key{kg.L, kg.d + 1, v};
+#pragma unroll
+    for (int a = 0; a < ND; a++) codes[a] = cg[a];
+    if (g + 1 == nk || key_le(mine, keys[g + 1])) {
+      *key_out = mine;
+      return v;
+    }
+    vprev = v;
+    kprev = mine;
+#pragma unroll
+    for (int a = 0; a < ND; a++) cprev[a] = cg[a];
+  }
+  *key_out = key_unreached();
+  return EIK_INF;
+}
+
+// Packed derivative codes: one byte per node, (c0+2) + 5*(c1+2) + 25*(c2+2) in the low
+// 7 bits; bit 7 marks a source point (traveltime fixed by the initialisation).
+EIK_HD uint8_t pack_codes(const int8_t* c, int nd) {
+  int v = (c[0] + 2) + 5 * (c[1] + 2);
+  if (nd == 3) v += 25 * (c[2] + 2);
+  else v += 25 * 2;
+  return (uint8_t)v;
+}
+EIK_HD void unpack_codes(uint8_t p, int8_t* c) {
+  int v = p & 0x7f;
+  c[0] = (int8_t)(v % 5 - 2);
+  c[1] = (int8_t)((v / 5) % 5 - 2);
+  c[2] = (int8_t)((v / 25) % 5 - 2);
+}
+constexpr uint8_t CODE_SRC_BIT = 0x80;
+constexpr uint8_t CODE_NONE = 2 + 5 * 2 + 25 * 2;  // all three codes zero
+
+}  // namespace eik

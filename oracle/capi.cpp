@@ -85,7 +85,8 @@ int eikor_forward_debug(int kind, const int64_t* grsize, const double* spacing,
                         int64_t ds, int64_t noderadius, double* tt, int8_t* codes,
                         int32_t* fmmpos, int64_t* srcpts, int64_t srcpts_cap, int64_t* stats,
                         int64_t* fine_n, int64_t fine_cap, double* fine_tt, uint8_t* fine_status,
-                        int32_t* fine_fmmpos, int64_t* fine_nacc, char* errbuf, int errlen) {
+                        int32_t* fine_fmmpos, int64_t* fine_nacc, int32_t* batch_out, char* errbuf,
+                        int errlen) {
   try {
     Grid g = make_grid(kind, grsize, spacing, cooinit);
     ExtraParams ep = make_ep(refine, ds, noderadius, 3, 0, 0, 1);
@@ -101,8 +102,12 @@ int eikor_forward_debug(int kind, const int64_t* grsize, const double* spacing,
     AdjointVars adjf;
     SrcRefinVars srv;
     FMMStats st;
+    std::vector<int32_t> batches;
+    if (batch_out) st.batch_of = &batches;
     ttFMM_hiord(fv, vel, src, &adj, ep, &fine, &adjf, &srv, &st);
     const int64_t N = g.npts();
+    if (batch_out)
+      for (int64_t i = 0; i < N; i++) batch_out[i] = batches.empty() ? -1 : batches[i];
     std::memcpy(tt, fv.ttime.data(), sizeof(double) * N);
     std::memcpy(codes, adj.code.data(), (size_t)(N * g.nd));
     for (int64_t i = 0; i < N; i++) fmmpos[i] = adj.lgrid2fmm[i];

@@ -163,6 +163,7 @@ struct SrcRefinVars {  // eikstructs.jl:492-500
 
 // Per-run counters used by tests and by the GPU-parity analysis.
 struct FMMStats {
+  std::vector<int32_t>* batch_of = nullptr;  // optional: batch index per coarse node (0 = source)
   i64 pops = 0;
   i64 nonmonotone_pops = 0;  // popped value smaller than an earlier popped value
   i64 max_batch = 0;

@@ -60,7 +60,7 @@ def lib():
                                      P, P, P, P, C.c_char_p, C.c_int]
         L.eikor_gradient.restype = C.c_int
         L.eikor_forward_debug.argtypes = [C.c_int, P, P, P, P, P, C.c_int, C.c_int64, C.c_int64, P,
-                                          P, P, P, C.c_int64, P, P, C.c_int64, P, P, P, P,
+                                          P, P, P, C.c_int64, P, P, C.c_int64, P, P, P, P, P,
                                           C.c_char_p, C.c_int]
         L.eikor_forward_debug.restype = C.c_int
         L.eikor_range_value.argtypes = [C.c_double, C.c_double, C.c_int64, C.c_int64]
@@ -205,16 +205,18 @@ def forward_debug(vel, grd, src, extraparams=None):
     fine_status = np.zeros(cap, dtype=np.uint8)
     fine_pos = np.zeros(cap, dtype=np.int32)
     fine_nacc = np.zeros(1, dtype=np.int64)
+    batch = np.zeros(N, dtype=np.int32)
     buf = C.create_string_buffer(512)
     src = np.ascontiguousarray(np.asarray(src, dtype=np.float64).ravel())
     rc = L.eikor_forward_debug(grd.kind, _p(gs), _p(sp), _p(co), _p(velf), _p(src), ep["refine"], ep["ds"],
                                ep["nr"], _p(tt), _p(codes), _p(fmmpos), _p(srcpts), srcpts.size, _p(stats),
                                _p(fine_n), cap, _p(fine_tt), _p(fine_status), _p(fine_pos), _p(fine_nacc),
-                               buf, 512)
+                               _p(batch), buf, 512)
     _check(rc, buf)
     out = dict(tt=tt.reshape(grd.grsize, order="F"), codes=codes.reshape(N, grd.ndim),
                fmmpos=fmmpos, srcpts=srcpts[:stats[3]].copy(), pops=int(stats[0]),
-               nonmonotone=int(stats[1]), max_batch=int(stats[2]), warn=int(stats[4]))
+               nonmonotone=int(stats[1]), max_batch=int(stats[2]), warn=int(stats[4]),
+               batch=batch.reshape(grd.grsize, order="F"))
     if ep["refine"]:
         fn = tuple(int(x) for x in fine_n[:grd.ndim])
         nf = int(np.prod(fn))

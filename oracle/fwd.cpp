@@ -665,9 +665,16 @@ void ttFMM_core(FMMVars& fv, const double* vel, AdjointVars* adj, FMMVars* coars
   bool firstwarning = true;
   std::vector<std::array<i64, 3>> popped;
   popped.reserve(128);
+  const bool rec_batch = st && st->batch_of && !refsrc;
+  if (rec_batch) {
+    st->batch_of->assign(N, -1);
+    for (i64 l = 0; l < naccinit; l++) (*st->batch_of)[g.lin(ijksrc[l].data())] = 0;
+  }
+  int32_t batchno = 0;
   for (i64 iter = 1; iter <= N - naccinit; iter++) {
     if (fv.bheap.Nh < 1) break;
     popped.clear();
+    batchno++;
     bool sameminval = true;
     while (sameminval) {
       node += 1;
@@ -681,6 +688,7 @@ void ttFMM_core(FMMVars& fv, const double* vel, AdjointVars* adj, FMMVars* coars
       g.cart_of(acchan, acc);
       fv.status[acchan] = 2;
       fv.ttime[acchan] = tmptt;
+      if (rec_batch) (*st->batch_of)[acchan] = batchno;
       if (st) {
         st->pops++;
         if (tmptt < maxpopped) st->nonmonotone_pops++;
