@@ -1,0 +1,491 @@
+// Host runtime of libeikcuda: contexts, resident velocity models, device scratch, and the
+// C-ABI entry points declared in include/eikcuda.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/eikcuda.h"
+#include "kernels.cuh"
+#include "runtime.hpp"
+
+namespace eik {
+
+thread_local std::string tl_error;
+
+int fail(eik_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  tl_error = buf;
+  (void)ctx;
+  return code;
+}
+
+#define CUDA_OK(ctx, call)                                                                      \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return fail(ctx, EIK_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));           \
+  } while (0)
+
+// -------------------------------------------------------------------- scratch --
+void* Scratch::get(const std::string& name, size_t bytes, int* rc) {
+  auto it = bufs.find(name);
+  if (it != bufs.end() && it->second.bytes >= bytes) return it->second.ptr;
+  if (it != bufs.end()) {
+    cudaFree(it->second.ptr);
+    total -= it->second.bytes;
+    bufs.erase(it);
+  }
+  if (total + bytes > budget) {
+    *rc = EIK_ERR_OUT_OF_BUDGET;
+    return nullptr;
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, std::max<size_t>(bytes, 256)) != cudaSuccess) {
+    *rc = EIK_ERR_CUDA;
+    return nullptr;
+  }
+  bufs[name] = Buf{p, bytes};
+  total += bytes;
+  return p;
+}
+void Scratch::release_all() {
+  for (auto& kv : bufs) cudaFree(kv.second.ptr);
+  bufs.clear();
+  total = 0;
+}
+
+// ----------------------------------------------------------------- grids --
+int make_griddesc(eik_ctx* ctx, const eik_grid* g, GridDesc* out) {
+  if (!g) return fail(ctx, EIK_ERR_ASSERT, "grid descriptor is NULL");
+  GridDesc d;
+  std::memset(&d, 0, sizeof d);
+  d.kind = g->kind;
+  const bool cart = g->kind == EIK_GRID2DCART || g->kind == EIK_GRID3DCART;
+  if (g->kind < 0 || g->kind > 3) return fail(ctx, EIK_ERR_ASSERT, "unknown grid kind %d", g->kind);
+  d.nd = (g->kind == EIK_GRID2DCART || g->kind == EIK_GRID2DSPHERE) ? 2 : 3;
+  if (g->ndim != d.nd) return fail(ctx, EIK_ERR_ASSERT, "2<=ndims(vel)<=3 / grid ndim mismatch");
+  for (int a = 0; a < 3; a++) {
+    d.n[a] = 1;
+    d.spac[a] = 0;
+    d.co[a] = 0;
+  }
+  for (int a = 0; a < d.nd; a++) {
+    if (g->grsize[a] <= 0) return fail(ctx, EIK_ERR_ASSERT, "all(grsize.>0)");
+    if (g->grsize[a] > (1 << 30)) return fail(ctx, EIK_ERR_UNSUPPORTED, "grid axis too large");
+    d.n[a] = (int32_t)g->grsize[a];
+    d.co[a] = g->cooinit[a];
+    d.spac[a] = cart ? g->spacing[0] : g->spacing[a];
+  }
+  if (cart && !(g->spacing[0] > 0.0)) return fail(ctx, EIK_ERR_ASSERT, "hgrid>0.0");
+  if (g->kind == EIK_GRID2DSPHERE) {
+    if (!(g->cooinit[0] >= 0.0)) return fail(ctx, EIK_ERR_ASSERT, "cooinit[1]>=0.0");
+    if (!(g->spacing[0] > 0.0)) return fail(ctx, EIK_ERR_ASSERT, "Δr>0.0");
+    if (!(g->spacing[1] > 0.0)) return fail(ctx, EIK_ERR_ASSERT, "Δθ>0.0");
+  }
+  if (g->kind == EIK_GRID3DSPHERE && !(g->cooinit[0] > 0.0)) return fail(ctx, EIK_ERR_ASSERT, "cooinit[1]>0.0");
+  for (int a = 0; a < d.nd; a++) d.ax[a] = make_jrange(d.co[a], d.spac[a]);
+  if (g->kind == EIK_GRID2DSPHERE) {
+    for (int i = 1; i <= d.n[1]; i++) {
+      const double th = jr_value(d.ax[1], i);
+      if (!(0.0 <= th && th <= 180.0)) return fail(ctx, EIK_ERR_ASSERT, "all(0.0.<=θ.<=180.0)");
+    }
+  } else if (g->kind == EIK_GRID3DSPHERE) {
+    for (int i = 1; i <= d.n[1]; i++) {
+      const double th = jr_value(d.ax[1], i);
+      if (!(5.0 <= th && th <= 175.0)) return fail(ctx, EIK_ERR_ASSERT, "all(5.0.<=θ.<=175.0)");
+    }
+    for (int i = 1; i <= d.n[2]; i++) {
+      const double ph = jr_value(d.ax[2], i);
+      if (!(0.0 <= ph && ph <= 180.0)) return fail(ctx, EIK_ERR_ASSERT, "all(0.0.<=φ.<=180.0)");
+    }
+  }
+  *out = d;
+  return EIK_OK;
+}
+
+// checksrcrecposition (src/EikSolv/eikchecks.jl:4-50)
+int check_positions(eik_ctx* ctx, const GridDesc& g, int64_t nsrc, const double* cs,
+                    const int64_t* recoff, const double* rec) {
+  for (int d = 0; d < g.nd; d++) {
+    const double lo = jr_value(g.ax[d], 1), hi = jr_value(g.ax[d], g.n[d]);
+    for (int64_t s = 0; s < nsrc; s++) {
+      const double x = cs[s * g.nd + d];
+      if (!(lo <= x && x <= hi))
+        return fail(ctx, EIK_ERR_ASSERT, "source %lld outside the grid on axis %d", (long long)s, d);
+    }
+    for (int64_t r = 0; r < recoff[nsrc]; r++) {
+      const double x = rec[r * g.nd + d];
+      if (!(lo <= x && x <= hi))
+        return fail(ctx, EIK_ERR_ASSERT, "receiver %lld outside the grid on axis %d", (long long)r, d);
+    }
+  }
+  for (int64_t s = 0; s < nsrc; s++)
+    if (recoff[s + 1] < recoff[s]) return fail(ctx, EIK_ERR_ASSERT, "rec_off must be non-decreasing");
+  return EIK_OK;
+}
+
+int check_extra(eik_ctx* ctx, const eik_extra* ep) {
+  if (ep->radiussmoothgradsrc < 0) return fail(ctx, EIK_ERR_ASSERT, "radiussmoothgradsrc>= 0");
+  if (ep->smoothgradkern < 0) return fail(ctx, EIK_ERR_ASSERT, "smoothgradkern>=0");
+  if (ep->smoothgradkern > 0 && ep->smoothgradkern % 2 == 0)
+    return fail(ctx, EIK_ERR_ERROR, "ExtraParams: smoothgradkern must be an odd number");
+  if (ep->parallelkind < 0 || ep->parallelkind > 2)
+    return fail(ctx, EIK_ERR_ERROR, "ExtraParams(): 'parallelkind' must be one of :serial, :sharedmem or :distribmem");
+  if (ep->refinearoundsrc && (ep->downscalefactor < 1 || ep->noderadius < 0))
+    return fail(ctx, EIK_ERR_ASSERT, "GridRefinementPars: downscalefactor>=1, noderadius>=0");
+  return EIK_OK;
+}
+
+__global__ void slowness_kernel(const double* vel, double* slow, long long n, int* nonpos) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = vel[i];
+    if (!(v > 0.0)) atomicExch(nonpos, 1);
+    slow[i] = 1.0 / v;
+  }
+}
+
+int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev, eik_model_id* out) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  Model m;
+  int rc = make_griddesc(ctx, grd, &m.g);
+  if (rc) return rc;
+  m.N = npts(m.g);
+  const size_t bytes = sizeof(double) * (size_t)m.N;
+  if (ctx->scratch.total + ctx->model_bytes + 2 * bytes > ctx->scratch.budget)
+    return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "model of %zu bytes exceeds the HBM budget", 2 * bytes);
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  CUDA_OK(ctx, cudaMalloc(&m.vel, bytes));
+  CUDA_OK(ctx, cudaMalloc(&m.slow, bytes));
+  if (dev) CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  else CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  int* dflag = nullptr;
+  CUDA_OK(ctx, cudaMalloc(&dflag, sizeof(int)));
+  CUDA_OK(ctx, cudaMemsetAsync(dflag, 0, sizeof(int), ctx->stream));
+  slowness_kernel<<<592, 256, 0, ctx->stream>>>(m.vel, m.slow, m.N, dflag);
+  int nonpos = 0;
+  CUDA_OK(ctx, cudaMemcpyAsync(&nonpos, dflag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(dflag);
+  if (nonpos) {
+    cudaFree(m.vel);
+    cudaFree(m.slow);
+    return fail(ctx, EIK_ERR_ASSERT, "all(vel.>0.0)");
+  }
+  ctx->model_bytes += 2 * bytes;
+  const eik_model_id id = ++ctx->next_model;
+  ctx->models[id] = m;
+  *out = id;
+  return EIK_OK;
+}
+
+uint32_t read_err(eik_ctx* ctx, uint32_t* derr) {
+  uint32_t h = 0;
+  cudaMemcpyAsync(&h, derr, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  return h;
+}
+
+int err_to_rc(eik_ctx* ctx, uint32_t e) {
+  if (!e) return EIK_OK;
+  if (e & ERRB_QUEUE_TIMEOUT) return fail(ctx, EIK_ERR_TIMEOUT, "device wait ran out (error word 0x%x)", e);
+  if (e & (ERRB_NOT_CONVERGED | ERRB_ADJ_NOT_CONVERGED))
+    return fail(ctx, EIK_ERR_NOT_CONVERGED, "iteration limit reached (error word 0x%x)", e);
+  if (e & ERRB_SINGULAR) return fail(ctx, EIK_ERR_ERROR, "SingularException in the adjoint solve");
+  return fail(ctx, EIK_ERR_UNSUPPORTED, "refined-grid capacity exceeded (error word 0x%x)", e);
+}
+
+// -------------------------------------------------------------- forward pipeline --
+// Runs the start-up stage and the coarse solve for nsrc sources whose coordinates,
+// receiver offsets and receivers are already on the device. On return the traveltimes of
+// source s are at fw.t + s*N (codes at fw.code + s*N).
+int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const eik_extra& ep,
+                   ForwardState* fw, eik_stats* stats) {
+  int rc = EIK_OK;
+  const GridDesc& g = m.g;
+  const long long N = m.N;
+  cudaStream_t st = ctx->stream;
+  Scratch& S = ctx->scratch;
+  ForwardBatch fb;
+  std::memset(&fb, 0, sizeof fb);
+  fb.g = g;
+  fb.nsrc = (int32_t)nsrc;
+  fb.ds = ep.downscalefactor;
+  fb.noderadius = ep.noderadius;
+  fb.vel = m.vel;
+  fb.slow = m.slow;
+  fb.coordsrc = d_cs;
+  const bool refine = ep.refinearoundsrc != 0;
+  long long win = 1, nfmax = 1;
+  for (int d = 0; d < g.nd; d++) {
+    win *= 2LL * ep.noderadius + 2;
+    nfmax *= (2LL * ep.noderadius + 1) * ep.downscalefactor + 1;
+  }
+  fb.seedcap = refine ? (int32_t)std::max<long long>(win, 8) : 8;
+  fb.nfmax = refine ? nfmax : 1;
+  fb.heapcap = (int32_t)std::min<long long>(refine ? nfmax : 1, 8192);
+#define GET(var, type, name, count)                                                  \
+  var = (type*)S.get(name, sizeof(type) * (size_t)(count), &rc);                     \
+  if (!var) return rc == EIK_ERR_OUT_OF_BUDGET                                       \
+                     ? fail(ctx, rc, "scratch '%s' exceeds the HBM budget", name)    \
+                     : fail(ctx, rc, "cudaMalloc of scratch '%s' failed", name);
+  GET(fb.out, SrcOut, "srcout", nsrc);
+  GET(fb.seed_lin, int32_t, "seed_lin", nsrc * fb.seedcap);
+  GET(fb.seed_tt, double, "seed_tt", nsrc * fb.seedcap);
+  GET(fb.err, uint32_t, "err", 4);
+  if (refine) {
+    GET(fb.fine_tt, double, "fine_tt", nsrc * fb.nfmax);
+    GET(fb.fine_status, uint8_t, "fine_status", nsrc * fb.nfmax);
+    GET(fb.fine_code, uint8_t, "fine_code", nsrc * fb.nfmax);
+    GET(fb.fine_idx, int32_t, "fine_idx", nsrc * fb.nfmax);
+    GET(fb.fine_order, int32_t, "fine_order", nsrc * fb.nfmax);
+    GET(fb.fine_onh, uint8_t, "fine_onh", nsrc * fb.nfmax);
+  }
+  // coarse problems
+  using C3 = int;  // tile extents per dimensionality
+  const int TX = g.nd == 3 ? 8 : 32, TY = g.nd == 3 ? 8 : 16, TZ = g.nd == 3 ? 8 : 1;
+  const int nt[3] = {(g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + TZ - 1) / TZ};
+  const long long tiles_per = (long long)nt[0] * nt[1] * nt[2];
+  double* t;
+  uint8_t* code;
+  double* kL;
+  uint8_t* kd;
+  GET(t, double, "t", nsrc * N);
+  GET(code, uint8_t, "code", nsrc * N);
+  GET(kL, double, "kL", nsrc * N);
+  GET(kd, uint8_t, "kd", nsrc * N);
+  std::vector<CoarseProblem> hp(nsrc);
+  for (int64_t s = 0; s < nsrc; s++) {
+    CoarseProblem& P = hp[s];
+    P.g = g;
+    P.slow = m.slow;
+    P.t = t + s * N;
+    P.code = code + s * N;
+    P.kL = kL + s * N;
+    P.kd = kd + s * N;
+    P.nt[0] = nt[0];
+    P.nt[1] = nt[1];
+    P.nt[2] = nt[2];
+    P.tbase = s * tiles_per;
+  }
+  CoarseProblem* dp;
+  GET(dp, CoarseProblem, "probs", nsrc);
+  SolveArgs sa;
+  std::memset(&sa, 0, sizeof sa);
+  sa.nprob = (int32_t)nsrc;
+  sa.nd = g.nd;
+  sa.ntiles = tiles_per * nsrc;
+  unsigned long long cap = 1;
+  while (cap < (unsigned long long)sa.ntiles) cap <<= 1;
+  sa.q.mask = cap - 1;
+  GET(sa.tile_faces, uint32_t, "tile_faces", sa.ntiles);
+  GET(sa.tile_flag, int32_t, "tile_flag", sa.ntiles);
+  GET(sa.q.items, unsigned long long, "q_items", cap);
+  GET(sa.q.seq, unsigned long long, "q_seq", cap);
+  unsigned long long* ctr;
+  GET(ctr, unsigned long long, "q_ctr", 8);
+  sa.q.head = ctr;
+  sa.q.tail = ctr + 1;
+  sa.activations = ctr + 2;
+  sa.node_evals = ctr + 3;
+  sa.pending = (int32_t*)(ctr + 4);
+  sa.abort_flag = (int32_t*)(ctr + 5);
+  sa.err = fb.err;
+  sa.probs = dp;
+  sa.max_activations = 400ull * (unsigned long long)sa.ntiles + 100000ull;
+  sa.max_passes = 64;
+  sa.timeout_ns = 20LL * 1000 * 1000 * 1000;
+#undef GET
+  CUDA_OK(ctx, cudaMemcpyAsync(dp, hp.data(), sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemsetAsync(fb.err, 0, sizeof(uint32_t) * 4, st));
+  CUDA_OK(ctx, cudaMemsetAsync(fb.out, 0, sizeof(SrcOut) * nsrc, st));
+  if (refine) launch_fine(fb, st);
+  else launch_srcbox(fb, st);
+  CUDA_OK(ctx, cudaGetLastError());
+  launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
+  CUDA_OK(ctx, cudaGetLastError());
+  launch_coarse_solve(sa, ctx->nsm, st);
+  CUDA_OK(ctx, cudaGetLastError());
+  fw->fb = fb;
+  fw->sa = sa;
+  fw->t = t;
+  fw->code = code;
+  fw->kL = kL;
+  fw->kd = kd;
+  fw->N = N;
+  fw->nsrc = nsrc;
+  (void)stats;
+  return EIK_OK;
+}
+
+int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
+  unsigned long long ctr[4] = {0, 0, 0, 0};
+  uint32_t e = 0;
+  cudaMemcpyAsync(ctr, fw->sa.q.head, sizeof ctr, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(&e, fw->fb.err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream);
+  std::vector<SrcOut> outs(fw->nsrc);
+  cudaMemcpyAsync(outs.data(), fw->fb.out, sizeof(SrcOut) * fw->nsrc, cudaMemcpyDeviceToHost, ctx->stream);
+  CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
+  uint32_t warn = 0;
+  for (auto& o : outs) warn |= o.warn;
+  if (stats) {
+    stats->warn_mask |= warn;
+    stats->err_mask |= e;
+    stats->tile_activations += ctr[2];
+    stats->node_evals += ctr[3];
+  }
+  fw->host_out = std::move(outs);
+  return err_to_rc(ctx, e);
+}
+
+}  // namespace eik
+
+using namespace eik;
+
+extern "C" {
+
+void eik_extra_defaults(eik_extra* ep) {
+  std::memset(ep, 0, sizeof *ep);
+  ep->refinearoundsrc = 1;
+  ep->downscalefactor = 5;
+  ep->noderadius = 3;
+  ep->radiussmoothgradsrc = 3;
+  ep->smoothgradkern = 0;
+  ep->parallelkind = 0;
+}
+
+int eik_ctx_create(int device, size_t hbm_budget, eik_ctx** out) {
+  if (!out) return fail(nullptr, EIK_ERR_ASSERT, "out is NULL");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(nullptr, EIK_ERR_CUDA, "no CUDA device available");
+  if (device < 0 || device >= ndev) return fail(nullptr, EIK_ERR_ASSERT, "device %d out of range", device);
+  if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, EIK_ERR_CUDA, "cudaSetDevice failed");
+  eik_ctx* c = new eik_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  c->nsm = prop.multiProcessorCount;
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  c->scratch.budget = hbm_budget ? hbm_budget : (size_t)(0.9 * (double)fr);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(nullptr, EIK_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+  *out = c;
+  return EIK_OK;
+}
+
+int eik_ctx_destroy(eik_ctx* ctx) {
+  if (!ctx) return EIK_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->models) {
+    cudaFree(kv.second.vel);
+    cudaFree(kv.second.slow);
+  }
+  ctx->scratch.release_all();
+  cudaEventDestroy(ctx->ev0);
+  cudaEventDestroy(ctx->ev1);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return EIK_OK;
+}
+
+const char* eik_last_error(eik_ctx* ctx) {
+  (void)ctx;
+  return tl_error.c_str();
+}
+
+int eik_model_upload(eik_ctx* ctx, const eik_grid* grd, const double* vel, eik_model_id* out) {
+  if (!ctx || !vel || !out) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  return model_create(ctx, grd, vel, false, out);
+}
+
+int eik_model_upload_device(eik_ctx* ctx, const eik_grid* grd, const double* vel_dev, eik_model_id* out) {
+  if (!ctx || !vel_dev || !out) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  return model_create(ctx, grd, vel_dev, true, out);
+}
+
+int eik_model_release(eik_ctx* ctx, eik_model_id model) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->models.find(model);
+  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(it->second.vel);
+  cudaFree(it->second.slow);
+  ctx->model_bytes -= 2 * sizeof(double) * (size_t)it->second.N;
+  ctx->models.erase(it);
+  return EIK_OK;
+}
+
+int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
+                   const int64_t* rec_off, const double* rec, const eik_extra* ep_in, double* picks,
+                   double* ttgrids, eik_stats* stats) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->models.find(model);
+  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  const Model& m = it->second;
+  eik_extra ep;
+  if (ep_in) ep = *ep_in;
+  else eik_extra_defaults(&ep);
+  int rc = check_extra(ctx, &ep);
+  if (rc) return rc;
+  if (nsrc < 0) return fail(ctx, EIK_ERR_ASSERT, "nsrc >= 0");
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  if (nsrc == 0) return EIK_OK;
+  if (!coordsrc || !rec_off || (!rec && rec_off[nsrc] > 0) || (!picks && rec_off[nsrc] > 0))
+    return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  rc = check_positions(ctx, m.g, nsrc, coordsrc, rec_off, rec);
+  if (rc) return rc;
+  for (int a = 0; a < m.g.nd; a++)
+    if (m.g.n[a] < 3) return fail(ctx, EIK_ERR_ERROR, "BoundsError: grid axis %d has fewer than 3 nodes", a);
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int nd = m.g.nd;
+  const long long nrec = rec_off[nsrc];
+  double* d_cs = (double*)ctx->scratch.get("in_cs", sizeof(double) * nsrc * nd, &rc);
+  long long* d_off = (long long*)ctx->scratch.get("in_off", sizeof(long long) * (nsrc + 1), &rc);
+  double* d_rec = (double*)ctx->scratch.get("in_rec", sizeof(double) * std::max<long long>(nrec, 1) * nd, &rc);
+  double* d_picks = (double*)ctx->scratch.get("out_picks", sizeof(double) * std::max<long long>(nrec, 1), &rc);
+  if (!d_cs || !d_off || !d_rec || !d_picks) return fail(ctx, rc, "scratch allocation failed");
+  cudaEventRecord(ctx->ev0, st);
+  CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
+  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
+  ForwardState fw;
+  rc = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
+  if (rc) return rc;
+  if (nrec) launch_picks(m.g, fw.t, m.N, (int)nsrc, d_off, d_rec, d_picks, st);
+  CUDA_OK(ctx, cudaGetLastError());
+  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
+  if (ttgrids)
+    CUDA_OK(ctx, cudaMemcpyAsync(ttgrids, fw.t, sizeof(double) * nsrc * m.N, cudaMemcpyDeviceToHost, st));
+  cudaEventRecord(ctx->ev1, st);
+  rc = collect_forward_stats(ctx, &fw, stats);
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->device_ms = ms;
+  }
+  return rc;
+}
+
+}  // extern "C"

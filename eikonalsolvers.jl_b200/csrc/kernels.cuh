@@ -1,0 +1,107 @@
+// Device-side interfaces between the kernels of libeikcuda and its host runtime.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace eik {
+
+// Refined-grid window of one source (createfinegrid, eikmainfwd.jl:950-1104), 0-based.
+struct FineInfo {
+  int32_t ds;
+  int32_t ijk1[3];    // coarse index of the window origin
+  int32_t nf[3];      // fine grid size
+  int32_t outmin[3];  // window clipped at the model's lower border on this axis
+  int32_t outmax[3];
+};
+
+// Per-source results of the start-up stage.
+struct SrcOut {
+  FineInfo fine;
+  int32_t nseeds;       // coarse source points (traveltimes fixed before the coarse solve)
+  int32_t nsrcf;        // source-box corners (of the fine grid if refined, else coarse)
+  int32_t nacc;         // accepted fine nodes at the stop (refined only)
+  uint32_t warn;
+  int32_t corn[8][3];   // source-box corners
+  double distcorn[8];
+  double velcorn[8];
+};
+
+struct ForwardBatch {
+  GridDesc g;               // coarse grid
+  int32_t nsrc;
+  int32_t ds, noderadius;
+  int32_t seedcap;          // capacity of seed lists per source
+  long long nfmax;          // capacity of fine arrays per source
+  int32_t heapcap;          // shared-memory heap capacity (fine FMM)
+  const double* vel;        // coarse velocity
+  const double* slow;       // 1/vel
+  const double* coordsrc;   // nsrc x nd
+  SrcOut* out;
+  int32_t* seed_lin;        // nsrc x seedcap: coarse node index
+  double* seed_tt;          // nsrc x seedcap
+  double* fine_tt;          // nsrc x nfmax
+  uint8_t* fine_status;
+  uint8_t* fine_code;
+  int32_t* fine_idx;        // heap handle positions
+  int32_t* fine_order;      // accepted fine nodes in FMM order
+  uint8_t* fine_onh;        // accepted fine node coincides with a coarse node
+  uint32_t* err;
+};
+
+// One coarse solve: a source on a grid. Several problems share one persistent launch.
+struct CoarseProblem {
+  GridDesc g;
+  const double* slow;
+  double* t;       // traveltime
+  uint8_t* code;   // packed derivative codes; bit 7: special key (source or non-causal)
+  double* kL;      // key level of special nodes (-inf for source points)
+  uint8_t* kd;     // key depth of special nodes
+  int32_t nt[3];   // tiles per axis
+  int32_t pad;
+  long long tbase; // first global tile id of this problem
+};
+
+// Bounded multi-producer/multi-consumer ring of tile ids (Vyukov's sequence scheme).
+struct TileQueue {
+  unsigned long long* items;
+  unsigned long long* seq;
+  unsigned long long* head;
+  unsigned long long* tail;
+  unsigned long long mask;
+};
+
+struct SolveArgs {
+  const CoarseProblem* probs;
+  int32_t nprob;
+  int32_t nd;
+  long long ntiles;            // total tiles over all problems
+  uint32_t* tile_faces;        // pending dirty faces per tile (bit 6: whole tile)
+  int32_t* tile_flag;          // 1 while queued
+  TileQueue q;
+  int32_t* pending;            // tiles queued or being processed
+  unsigned long long* activations;
+  unsigned long long max_activations;
+  unsigned long long* node_evals;
+  uint32_t* err;
+  int32_t* abort_flag;
+  int32_t max_passes;
+  long long timeout_ns;
+};
+
+constexpr uint32_t FACES_ALL = 1u << 6;
+
+// launchers (defined in the .cu files)
+void launch_srcbox(const ForwardBatch& fb, cudaStream_t st);
+void launch_fine(const ForwardBatch& fb, cudaStream_t st);
+size_t fine_smem_bytes(int heapcap);
+void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs, int nprob,
+                        const ForwardBatch& fb, const SolveArgs& sa, cudaStream_t st);
+void launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
+void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
+                  const double* rec, double* picks, cudaStream_t st);
+
+}  // namespace eik

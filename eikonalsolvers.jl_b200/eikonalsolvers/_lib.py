@@ -1,0 +1,123 @@
+"""ctypes binding of libeikcuda.so (include/eikcuda.h).
+
+The library is built in-tree (``eikonalsolvers.jl_b200/build.py``) and loaded from
+``eikonalsolvers.jl_b200/lib``. There is no CPU path: loading fails loudly when the
+library is missing, and the first call fails when no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(os.path.dirname(_HERE), "lib", "libeikcuda.so")
+
+EIK_OK = 0
+ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EIK_ERR_NOT_CONVERGED",
+          -5: "EIK_ERR_OUT_OF_BUDGET", -6: "EIK_ERR_TIMEOUT", -7: "EIK_ERR_UNSUPPORTED"}
+
+EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last_error",
+            "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
+            "eik_gradient"]
+
+
+class EikError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class EikAssertionError(EikError, AssertionError):
+    pass
+
+
+class eik_grid(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("ndim", C.c_int32), ("grsize", C.c_int64 * 3),
+                ("spacing", C.c_double * 3), ("cooinit", C.c_double * 3)]
+
+
+class eik_extra(C.Structure):
+    _fields_ = [("refinearoundsrc", C.c_int32), ("downscalefactor", C.c_int32),
+                ("noderadius", C.c_int32), ("radiussmoothgradsrc", C.c_int32),
+                ("smoothgradkern", C.c_int32), ("parallelkind", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
+
+
+class eik_stats(C.Structure):
+    _fields_ = [("warn_mask", C.c_uint32), ("err_mask", C.c_uint32), ("tile_activations", C.c_uint64),
+                ("node_evals", C.c_uint64), ("device_ms", C.c_double)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load libeikcuda.so (building it first when the sources are newer)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIBPATH):
+            raise ImportError(f"libeikcuda.so not found at {LIBPATH}; run eikonalsolvers.jl_b200/build.py")
+        L = C.CDLL(LIBPATH)
+        P = C.c_void_p
+        L.eik_extra_defaults.argtypes = [C.POINTER(eik_extra)]
+        L.eik_extra_defaults.restype = None
+        L.eik_ctx_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(P)]
+        L.eik_ctx_destroy.argtypes = [P]
+        L.eik_last_error.argtypes = [P]
+        L.eik_last_error.restype = C.c_char_p
+        L.eik_model_upload.argtypes = [P, C.POINTER(eik_grid), P, C.POINTER(C.c_int64)]
+        L.eik_model_upload_device.argtypes = [P, C.POINTER(eik_grid), P, C.POINTER(C.c_int64)]
+        L.eik_model_release.argtypes = [P, C.c_int64]
+        L.eik_traveltime.argtypes = [P, C.c_int64, C.c_int64, P, P, P, C.POINTER(eik_extra), P, P,
+                                     C.POINTER(eik_stats)]
+        L.eik_gradient.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, C.c_int32,
+                                   C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
+        for f in ("eik_ctx_create", "eik_ctx_destroy", "eik_model_upload", "eik_model_upload_device",
+                  "eik_model_release", "eik_traveltime", "eik_gradient"):
+            getattr(L, f).restype = C.c_int
+        _lib = L
+        return L
+
+
+def check(rc: int, ctx=None):
+    if rc == EIK_OK:
+        return
+    msg = load().eik_last_error(ctx).decode(errors="replace")
+    if rc == -1:
+        raise EikAssertionError(rc, msg)
+    raise EikError(rc, msg)
+
+
+def ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def grid_struct(grd) -> eik_grid:
+    g = eik_grid()
+    g.kind = grd.kind
+    g.ndim = grd.ndim
+    sp = list(grd.spacing) + [0.0] * (3 - grd.ndim)
+    for a in range(3):
+        g.grsize[a] = grd.grsize[a] if a < grd.ndim else 1
+        g.cooinit[a] = grd.cooinit[a] if a < grd.ndim else 0.0
+        g.spacing[a] = sp[a]
+    return g
+
+
+def extra_struct(extraparams) -> eik_extra:
+    e = eik_extra()
+    load().eik_extra_defaults(C.byref(e))
+    if extraparams is not None:
+        e.refinearoundsrc = int(extraparams.refinearoundsrc)
+        e.downscalefactor = int(extraparams.grdrefpars.downscalefactor)
+        e.noderadius = int(extraparams.grdrefpars.noderadius)
+        e.radiussmoothgradsrc = int(extraparams.radiussmoothgradsrc)
+        e.smoothgradkern = int(extraparams.smoothgradkern)
+        e.parallelkind = {"serial": 0, "sharedmem": 1, "distribmem": 2}[extraparams.parallelkind]
+    return e

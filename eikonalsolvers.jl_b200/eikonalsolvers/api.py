@@ -1,0 +1,179 @@
+"""Public API of EikonalSolvers.jl over libeikcuda, with the reference's signatures:
+
+* ``eiktraveltime(vel, grd, coordsrc, coordrec; returntt, extraparams)``
+  (src/EikSolv/eikmainfwd.jl:33-143)
+* ``eikgradient(vel, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad; extraparams)``
+  (src/EikSolv/eikmaingrad.jl:31-164)
+* ``eikttimemisfit(velmod, grd, coordsrc, coordrec, ttpicksobs, stdobs; extraparams)``
+  (src/EikSolv/eikmaingrad.jl:1302-1328)
+
+Arrays follow the reference: ``vel[i, j(, k)]`` indexed by grid node (x fastest in
+memory order is handled here), ``coordsrc`` is (nsrc, ndim), ``coordrec`` a list of
+(nrec_s, ndim) arrays, picks are returned as a list of 1-D arrays. Assertion failures of
+the reference raise ``AssertionError``; its ``error()`` calls raise ``RuntimeError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .structs import WHICHGRAD, ExtraParams, normalize_inputs
+
+
+class Context:
+    """A libeikcuda context on one CUDA device (stream, resident models, HBM budget)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.L = _lib.load()
+        self.h = C.c_void_p()
+        _lib.check(self.L.eik_ctx_create(int(device), C.c_size_t(int(hbm_budget)), C.byref(self.h)))
+        self.device = device
+        self.last_stats = _lib.eik_stats()
+
+    def close(self):
+        if self.h:
+            self.L.eik_ctx_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- models --
+    def upload(self, vel: np.ndarray, grd) -> int:
+        """Upload a velocity model (kept resident until ``release``); returns its id."""
+        vel = np.asarray(vel, dtype=np.float64)
+        assert tuple(vel.shape) == tuple(grd.grsize), "size(vel)==grd.grsize"
+        velf = np.ascontiguousarray(np.asfortranarray(vel).ravel(order="F"))
+        g = _lib.grid_struct(grd)
+        mid = C.c_int64()
+        _lib.check(self.L.eik_model_upload(self.h, C.byref(g), _lib.ptr(velf), C.byref(mid)), self.h)
+        return mid.value
+
+    def upload_device(self, vel_dev_ptr: int, grd) -> int:
+        """Upload a model from a device pointer (column-major FP64) of this context's GPU."""
+        g = _lib.grid_struct(grd)
+        mid = C.c_int64()
+        _lib.check(self.L.eik_model_upload_device(self.h, C.byref(g), C.c_void_p(vel_dev_ptr), C.byref(mid)),
+                   self.h)
+        return mid.value
+
+    def release(self, model: int):
+        _lib.check(self.L.eik_model_release(self.h, C.c_int64(model)), self.h)
+
+    # ------------------------------------------------------------------ calls --
+    def traveltime(self, model: int, grd, coordsrc, coordrec, returntt=False, extraparams=None):
+        cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+        if isinstance(coordrec, np.ndarray) and coordrec.dtype != object:
+            coordrec = [coordrec]
+        recs = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+        assert cs.shape[0] == len(recs), "size(coordsrc,1)==length(coordrec)"
+        recoff = np.zeros(len(recs) + 1, dtype=np.int64)
+        for s, r in enumerate(recs):
+            recoff[s + 1] = recoff[s] + r.shape[0]
+        rec = np.ascontiguousarray(np.concatenate(recs, axis=0)) if recs else np.zeros((0, grd.ndim))
+        nsrc = cs.shape[0]
+        picks = np.zeros(int(recoff[-1]), dtype=np.float64)
+        N = int(np.prod(grd.grsize))
+        ttg = np.zeros(nsrc * N, dtype=np.float64) if returntt else None
+        ep = _lib.extra_struct(extraparams)
+        st = _lib.eik_stats()
+        rc = self.L.eik_traveltime(self.h, C.c_int64(model), nsrc, _lib.ptr(cs), _lib.ptr(recoff), _lib.ptr(rec),
+                                   C.byref(ep), _lib.ptr(picks), _lib.ptr(ttg), C.byref(st))
+        self.last_stats = st
+        _lib.check(rc, self.h)
+        out = [picks[recoff[s]:recoff[s + 1]].copy() for s in range(nsrc)]
+        if returntt:
+            return out, [ttg[s * N:(s + 1) * N].reshape(grd.grsize, order="F").copy() for s in range(nsrc)]
+        return out
+
+    def gradient(self, model: int, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad, extraparams=None):
+        wg = whichgrad.lstrip(":") if isinstance(whichgrad, str) else whichgrad
+        assert wg in WHICHGRAD, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)"
+        cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+        if isinstance(coordrec, np.ndarray) and coordrec.dtype != object:
+            coordrec = [coordrec]
+        recs = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+        nsrc = cs.shape[0]
+        assert len(recs) == len(pickobs), "length(coordrec)==length(pickobs)"
+        for r, p, s in zip(recs, pickobs, stdobs):
+            assert r.shape[0] == np.asarray(p).shape[0], "size(coordrec[r],1)==size(pickobs[r],1)"
+            assert np.asarray(s).shape == np.asarray(p).shape, "size(stdobs[r])==size(pickobs[r])"
+        recoff = np.zeros(len(recs) + 1, dtype=np.int64)
+        for s, r in enumerate(recs):
+            recoff[s + 1] = recoff[s] + r.shape[0]
+        rec = np.ascontiguousarray(np.concatenate(recs, axis=0)) if recs else np.zeros((0, grd.ndim))
+        po = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).ravel() for p in pickobs]))
+        so = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).ravel() for p in stdobs]))
+        N = int(np.prod(grd.grsize))
+        gv = np.zeros(N, dtype=np.float64) if wg in ("gradvel", "gradvelandsrcloc") else None
+        gs = np.zeros(nsrc * grd.ndim, dtype=np.float64) if wg in ("gradsrcloc", "gradvelandsrcloc") else None
+        misf = np.zeros(1, dtype=np.float64)
+        ep = _lib.extra_struct(extraparams)
+        st = _lib.eik_stats()
+        rc = self.L.eik_gradient(self.h, C.c_int64(model), nsrc, _lib.ptr(cs), _lib.ptr(recoff), _lib.ptr(rec),
+                                 _lib.ptr(po), _lib.ptr(so), WHICHGRAD[wg], C.byref(ep), _lib.ptr(gv),
+                                 _lib.ptr(gs), _lib.ptr(misf), C.byref(st))
+        self.last_stats = st
+        _lib.check(rc, self.h)
+        gradvel = gv.reshape(grd.grsize, order="F") if gv is not None else None
+        gradsrc = gs.reshape(nsrc, grd.ndim) if gs is not None else None
+        if wg == "gradvel":
+            return gradvel, float(misf[0])
+        if wg == "gradsrcloc":
+            return gradsrc, float(misf[0])
+        return gradvel, gradsrc, float(misf[0])
+
+
+_default: dict = {}
+_dlock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _dlock:
+        if device not in _default:
+            _default[device] = Context(device)
+        return _default[device]
+
+
+def _with_model(vel, grd, fn, ctx: Optional[Context] = None):
+    ctx = ctx or default_context()
+    mid = ctx.upload(vel, grd)
+    try:
+        return fn(ctx, mid)
+    finally:
+        ctx.release(mid)
+
+
+def eiktraveltime(vel, grd, coordsrc, coordrec, returntt: bool = False,
+                  extraparams: Optional[ExtraParams] = None, ctx: Optional[Context] = None):
+    """Traveltimes at the receivers (and optionally on the whole grid) for every source."""
+    vel = np.asarray(vel, dtype=np.float64)
+    assert 2 <= vel.ndim <= 3, "2<=ndims(vel)<=3"
+    return _with_model(vel, grd, lambda c, m: c.traveltime(m, grd, coordsrc, coordrec, returntt, extraparams), ctx)
+
+
+def eikgradient(vel, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad,
+                extraparams: Optional[ExtraParams] = None, ctx: Optional[Context] = None):
+    """Gradient of the misfit w.r.t. velocity and/or source location, plus the misfit."""
+    vel = np.asarray(vel, dtype=np.float64)
+    assert 2 <= vel.ndim <= 3, "2<=ndims(vel)<=3"
+    return _with_model(vel, grd, lambda c, m: c.gradient(m, grd, coordsrc, coordrec, pickobs, stdobs,
+                                                         whichgrad, extraparams), ctx)
+
+
+def eikttimemisfit(velmod, grd, coordsrc, coordrec, ttpicksobs, stdobs,
+                   extraparams: Optional[ExtraParams] = None, ctx: Optional[Context] = None) -> float:
+    """0.5 * Σ_s Σ_r (t - obs)² / σ² through eiktraveltime (eikmaingrad.jl:1302-1328)."""
+    picks = eiktraveltime(velmod, grd, coordsrc, coordrec, extraparams=extraparams, ctx=ctx)
+    misf = 0.0
+    for s in range(len(picks)):
+        d = picks[s] - np.asarray(ttpicksobs[s])
+        misf += float(np.sum(d * d / np.asarray(stdobs[s]) ** 2))
+    return 0.5 * misf

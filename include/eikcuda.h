@@ -1,0 +1,131 @@
+/*
+ * libeikcuda: B200 (sm_100a) implementation of the forward and discrete-adjoint hot path
+ * of EikonalSolvers.jl 0.15.3, behind a plain C ABI.
+ *
+ * The reference has no FFI of its own (it is pure Julia); the seam these entry points
+ * replace is the per-source-group worker pair that all three `parallelkind` branches call:
+ *   ttforwsomesrc   (src/EikSolv/eikmainfwd.jl:152-199)  -> eik_traveltime
+ *   calcgradsomesrc (src/EikSolv/eikmaingrad.jl:174-258) -> eik_gradient
+ * so that the public Julia API keeps its signatures:
+ *   eiktraveltime  (src/EikSolv/eikmainfwd.jl:33-143)
+ *   eikgradient    (src/EikSolv/eikmaingrad.jl:31-164)
+ *   eikttimemisfit (src/EikSolv/eikmaingrad.jl:1302-1328)
+ *
+ * Conventions
+ *  - Arrays are FP64. Grids are column-major with x fastest (Julia's layout, cart2lin in
+ *    src/EikSolv/eikutils.jl:6-19); indices in this ABI are 0-based.
+ *  - coordsrc is nsrc x ndim row-major (source s at coordsrc[s*ndim .. s*ndim+ndim-1]).
+ *  - Receivers of all sources are concatenated row-major; rec_off[0..nsrc] are offsets
+ *    (receiver r of source s is row rec_off[s]+r). Picks, pickobs and stdobs follow rec_off.
+ *  - Spherical grids take θ, φ in degrees, as the reference.
+ *  - All host buffers are caller-owned; outputs are preallocated by the caller.
+ *    Device memory is owned by the context; models stay resident until released.
+ *  - Return value: EIK_OK or a negative EIK_ERR_*; eik_last_error() gives the message of
+ *    the calling thread's last failure on that context.
+ */
+#ifndef EIKCUDA_H
+#define EIKCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EIK_OK 0
+#define EIK_ERR_ASSERT (-1)        /* an @assert of the reference failed (AssertionError) */
+#define EIK_ERR_ERROR (-2)         /* an error() call of the reference (ErrorException) */
+#define EIK_ERR_CUDA (-3)          /* CUDA runtime failure */
+#define EIK_ERR_NOT_CONVERGED (-4) /* iteration limit reached */
+#define EIK_ERR_OUT_OF_BUDGET (-5) /* request does not fit the context's HBM budget */
+#define EIK_ERR_TIMEOUT (-6)       /* a bounded device wait ran out */
+#define EIK_ERR_UNSUPPORTED (-7)   /* configuration outside what this build implements */
+
+/* Grid kinds (src/EikSolv/eikstructs.jl:33-219). */
+#define EIK_GRID2DCART 0
+#define EIK_GRID3DCART 1
+#define EIK_GRID2DSPHERE 2
+#define EIK_GRID3DSPHERE 3
+
+/* whichgrad (eikmaingrad.jl:40): :gradvel, :gradsrcloc, :gradvelandsrcloc */
+#define EIK_GRADVEL 1
+#define EIK_GRADSRCLOC 2
+#define EIK_GRADVELANDSRCLOC 3
+
+/* Warning bits (the reference's @warn sites). */
+#define EIK_WARN_NEG_DISCRIMINANT 0x1u     /* eikforward2D.jl:342 / eikforward3D.jl:429 */
+#define EIK_WARN_SRC_HALFWAY_SHIFT 0x2u    /* eikmainfwd.jl:1298 */
+#define EIK_WARN_BORDER_BEFORE_COARSE 0x4u /* eikmainfwd.jl:731 */
+#define EIK_WARN_SRCPOS_ALIGNED_SHIFT 0x8u /* eikmaingrad.jl:1250 */
+#define EIK_WARN_SRC_ON_NODE_DERIV 0x10u   /* eikmaingrad.jl:1260 */
+#define EIK_WARN_FINE_NO_TRIGGER 0x20u     /* refined grid covered the model: no edge stop */
+
+typedef struct eik_ctx eik_ctx;
+typedef int64_t eik_model_id;
+
+/* Grid2DCart/Grid3DCart: spacing = {hgrid, hgrid, hgrid};
+ * Grid2DSphere: {Δr, Δθ, -}; Grid3DSphere: {Δr, Δθ, Δφ}. Unused entries are ignored. */
+typedef struct {
+  int32_t kind;
+  int32_t ndim;
+  int64_t grsize[3];
+  double spacing[3];
+  double cooinit[3];
+} eik_grid;
+
+/* ExtraParams / GridRefinementPars (src/EikSolv/eikstructs.jl:230-282). parallelkind is
+ * accepted and ignored: every call batches all its sources on the device. */
+typedef struct {
+  int32_t refinearoundsrc;      /* default 1 */
+  int32_t downscalefactor;      /* default 5 */
+  int32_t noderadius;           /* default 3 */
+  int32_t radiussmoothgradsrc;  /* default 3 */
+  int32_t smoothgradkern;       /* default 0 (odd when > 0) */
+  int32_t parallelkind;         /* 0 serial, 1 sharedmem, 2 distribmem */
+  int32_t reserved[2];
+} eik_extra;
+
+typedef struct {
+  uint32_t warn_mask;        /* EIK_WARN_* */
+  uint32_t err_mask;         /* device error word of the last launch (0 = none) */
+  uint64_t tile_activations; /* coarse tiles processed */
+  uint64_t node_evals;       /* coarse node updates evaluated */
+  double device_ms;          /* device time of the call (CUDA events) */
+} eik_stats;
+
+/* Fills the reference defaults of ExtraParams(). */
+void eik_extra_defaults(eik_extra* ep);
+
+/* Creates a context on CUDA device `device`. hbm_budget bounds the device memory the
+ * context may hold (0 = 90% of the device's free memory). */
+int eik_ctx_create(int device, size_t hbm_budget, eik_ctx** out);
+int eik_ctx_destroy(eik_ctx* ctx);
+const char* eik_last_error(eik_ctx* ctx);
+
+/* Uploads a velocity model (host, column-major, FP64) and keeps it resident. Checks
+ * all(vel.>0) (eikmainfwd.jl:45). */
+int eik_model_upload(eik_ctx* ctx, const eik_grid* grd, const double* vel, eik_model_id* out);
+/* Same, from a device pointer of this context's device. */
+int eik_model_upload_device(eik_ctx* ctx, const eik_grid* grd, const double* vel_dev, eik_model_id* out);
+int eik_model_release(eik_ctx* ctx, eik_model_id model);
+
+/* Replaces ttforwsomesrc (eikmainfwd.jl:152-199) for all nsrc sources at once.
+ * picks: rec_off[nsrc] values. ttgrids: nullable, nsrc x N traveltime grids (returntt). */
+int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
+                   const int64_t* rec_off, const double* rec, const eik_extra* ep, double* picks,
+                   double* ttgrids, eik_stats* stats);
+
+/* Replaces calcgradsomesrc (eikmaingrad.jl:174-258) with the sources in one group (the
+ * :serial order). gradvel: nullable N values; gradsrc: nullable nsrc x ndim; misfit: the
+ * summed 0.5*Σ(t-obs)²/σ² of the group. */
+int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
+                 const int64_t* rec_off, const double* rec, const double* pickobs,
+                 const double* stdobs, int32_t whichgrad, const eik_extra* ep, double* gradvel,
+                 double* gradsrc, double* misfit, eik_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EIKCUDA_H */
