@@ -148,12 +148,15 @@ int check_extra(eik_ctx* ctx, const eik_extra* ep) {
   return EIK_OK;
 }
 
-__global__ void slowness_kernel(const double* vel, double* slow, long long n, int* nonpos) {
+__global__ void slowness_kernel(const double* vel, double* slow, long long n, int* nonpos, double* ssum) {
+  double acc = 0.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double v = vel[i];
     if (!(v > 0.0)) atomicExch(nonpos, 1);
     slow[i] = 1.0 / v;
+    acc += (v > 0.0) ? 1.0 / v : 0.0;
   }
+  atomicAdd(ssum, acc);
 }
 
 int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev, eik_model_id* out) {
@@ -171,13 +174,25 @@ int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev,
   if (dev) CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   else CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyHostToDevice, ctx->stream));
   int* dflag = nullptr;
-  CUDA_OK(ctx, cudaMalloc(&dflag, sizeof(int)));
-  CUDA_OK(ctx, cudaMemsetAsync(dflag, 0, sizeof(int), ctx->stream));
-  slowness_kernel<<<592, 256, 0, ctx->stream>>>(m.vel, m.slow, m.N, dflag);
+  CUDA_OK(ctx, cudaMalloc(&dflag, 2 * sizeof(double)));
+  CUDA_OK(ctx, cudaMemsetAsync(dflag, 0, 2 * sizeof(double), ctx->stream));
+  double* dsum = reinterpret_cast<double*>(dflag) + 1;
+  slowness_kernel<<<592, 256, 0, ctx->stream>>>(m.vel, m.slow, m.N, dflag, dsum);
   int nonpos = 0;
+  double ssum = 0.0;
   CUDA_OK(ctx, cudaMemcpyAsync(&nonpos, dflag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_OK(ctx, cudaMemcpyAsync(&ssum, dsum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
   cudaFree(dflag);
+  {
+    // time scale for scheduling only: grid diagonal x mean slowness
+    double dh[3];
+    node_dh(m.g, m.g.n[0] / 2, dh);
+    double diag2 = 0.0;
+    for (int a = 0; a < m.g.nd; a++) diag2 += (double)m.g.n[a] * dh[a] * (double)m.g.n[a] * dh[a];
+    m.tscale = sqrt(diag2) * (ssum / (double)m.N);
+    if (!(m.tscale > 0.0) || !std::isfinite(m.tscale)) m.tscale = 1.0;
+  }
   if (nonpos) {
     cudaFree(m.vel);
     cudaFree(m.slow);
@@ -254,7 +269,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   }
   // coarse problems
   using C3 = int;  // tile extents per dimensionality
-  const int TX = g.nd == 3 ? 8 : 32, TY = g.nd == 3 ? 8 : 16, TZ = g.nd == 3 ? 8 : 1;
+  const int TX = g.nd == 3 ? 4 : 8, TY = g.nd == 3 ? 4 : 8, TZ = g.nd == 3 ? 4 : 1;
   const int nt[3] = {(g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + TZ - 1) / TZ};
   const long long tiles_per = (long long)nt[0] * nt[1] * nt[2];
   double* t;
@@ -278,6 +293,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     P.nt[1] = nt[1];
     P.nt[2] = nt[2];
     P.tbase = s * tiles_per;
+    P.tinv = (double)QBUCKETS / m.tscale;
   }
   CoarseProblem* dp;
   GET(dp, CoarseProblem, "probs", nsrc);
@@ -286,25 +302,29 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   sa.nprob = (int32_t)nsrc;
   sa.nd = g.nd;
   sa.ntiles = tiles_per * nsrc;
+  // per-bucket ring capacity: the front occupies a small fraction of all tiles at a time
   unsigned long long cap = 1;
-  while (cap < (unsigned long long)sa.ntiles) cap <<= 1;
+  const unsigned long long want = std::max<unsigned long long>((unsigned long long)sa.ntiles / 16, 1ull << 16);
+  while (cap < want) cap <<= 1;
   sa.q.mask = cap - 1;
   GET(sa.tile_faces, uint32_t, "tile_faces", sa.ntiles);
   GET(sa.tile_flag, int32_t, "tile_flag", sa.ntiles);
-  GET(sa.q.items, unsigned long long, "q_items", cap);
-  GET(sa.q.seq, unsigned long long, "q_seq", cap);
+  GET(sa.q.items, unsigned long long, "q_items", cap * QBUCKETS);
+  GET(sa.q.seq, unsigned long long, "q_seq", cap * QBUCKETS);
+  GET(sa.tile_prio, unsigned long long, "tile_prio", sa.ntiles);
   unsigned long long* ctr;
-  GET(ctr, unsigned long long, "q_ctr", 8);
+  GET(ctr, unsigned long long, "q_ctr", 2 * QBUCKETS + 8);
   sa.q.head = ctr;
-  sa.q.tail = ctr + 1;
-  sa.activations = ctr + 2;
-  sa.node_evals = ctr + 3;
-  sa.pending = (int32_t*)(ctr + 4);
-  sa.abort_flag = (int32_t*)(ctr + 5);
+  sa.q.tail = ctr + QBUCKETS;
+  sa.activations = ctr + 2 * QBUCKETS;
+  sa.node_evals = ctr + 2 * QBUCKETS + 1;
+  sa.pending = (int32_t*)(ctr + 2 * QBUCKETS + 2);
+  sa.abort_flag = (int32_t*)(ctr + 2 * QBUCKETS + 3);
   sa.err = fb.err;
   sa.probs = dp;
   sa.max_activations = 400ull * (unsigned long long)sa.ntiles + 100000ull;
-  sa.max_passes = 64;
+  sa.max_passes = 4096;
+  sa.gate = 1.0;
   sa.timeout_ns = 20LL * 1000 * 1000 * 1000;
 #undef GET
   CUDA_OK(ctx, cudaMemcpyAsync(dp, hp.data(), sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
@@ -332,7 +352,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
 int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
   unsigned long long ctr[4] = {0, 0, 0, 0};
   uint32_t e = 0;
-  cudaMemcpyAsync(ctr, fw->sa.q.head, sizeof ctr, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(ctr + 2, fw->sa.activations, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream);
   cudaMemcpyAsync(&e, fw->fb.err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream);
   std::vector<SrcOut> outs(fw->nsrc);
   cudaMemcpyAsync(outs.data(), fw->fb.out, sizeof(SrcOut) * fw->nsrc, cudaMemcpyDeviceToHost, ctx->stream);

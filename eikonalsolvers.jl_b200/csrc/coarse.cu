@@ -24,12 +24,15 @@ __device__ __forceinline__ long long gtimer_ns() {
   return t;
 }
 
-// Push; the caller guarantees at most (mask+1) items are ever in the queue at once.
-__device__ bool q_push(const SolveArgs& a, unsigned long long item) {
-  const unsigned long long pos = atomicAdd(a.q.tail, 1ull);
+// Push into bucket b; the caller guarantees at most (mask+1) items are ever in one bucket.
+__device__ bool q_push(const SolveArgs& a, int b, unsigned long long item) {
+  const unsigned long long cap = a.q.mask + 1;
+  unsigned long long* seq = a.q.seq + (unsigned long long)b * cap;
+  unsigned long long* items = a.q.items + (unsigned long long)b * cap;
+  const unsigned long long pos = atomicAdd(a.q.tail + b, 1ull);
   const unsigned long long slot = pos & a.q.mask;
   const long long t0 = gtimer_ns();
-  while (ld_volatile(a.q.seq + slot) != pos) {
+  while (ld_volatile(seq + slot) != pos) {
     if (gtimer_ns() - t0 > a.timeout_ns) {
       atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
       atomicExch(a.abort_flag, 1);
@@ -37,34 +40,74 @@ __device__ bool q_push(const SolveArgs& a, unsigned long long item) {
     }
     __nanosleep(64);
   }
-  a.q.items[slot] = item;
+  items[slot] = item;
   __threadfence();
-  atomicExch(a.q.seq + slot, pos + 1);
+  atomicExch(seq + slot, pos + 1);
   return true;
 }
 
-// Try to pop; returns false when the queue looks empty.
-__device__ bool q_pop(const SolveArgs& a, unsigned long long* item) {
-  for (;;) {
-    const unsigned long long h = ld_volatile(a.q.head);
-    const unsigned long long t = ld_volatile(a.q.tail);
-    if (h >= t) return false;
-    if (atomicCAS(a.q.head, h, h + 1) != h) continue;
-    const unsigned long long slot = h & a.q.mask;
-    const long long t0 = gtimer_ns();
-    while (ld_volatile(a.q.seq + slot) != h + 1) {
-      if (gtimer_ns() - t0 > a.timeout_ns) {
-        atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
-        atomicExch(a.abort_flag, 1);
-        return false;
+// Warp-cooperative pop of up to QCLAIM items from the lowest non-empty bucket with one CAS
+// (called by all lanes of one warp; results valid in every lane). Returns the count (0 when
+// every bucket looks empty).
+constexpr int QCLAIM = 4;
+__device__ int q_pop_warp(const SolveArgs& a, unsigned long long* items_out) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long cap = a.q.mask + 1;
+  for (int attempt = 0; attempt < 4096; attempt++) {
+    const int b0 = lane, b1 = lane + 32;
+    const unsigned long long h0 = ld_volatile(a.q.head + b0), t0v = ld_volatile(a.q.tail + b0);
+    const unsigned long long h1 = ld_volatile(a.q.head + b1), t1v = ld_volatile(a.q.tail + b1);
+    const unsigned m0 = __ballot_sync(0xffffffffu, h0 < t0v), m1 = __ballot_sync(0xffffffffu, h1 < t1v);
+    if (!m0 && !m1) return 0;
+    const int b = m0 ? __ffs(m0) - 1 : 32 + __ffs(m1) - 1;
+    int got = 0;
+    if (lane == 0) {
+      const unsigned long long h = ld_volatile(a.q.head + b), t = ld_volatile(a.q.tail + b);
+      if (h < t) {
+        const unsigned long long k = (t - h) < (unsigned long long)QCLAIM ? (t - h) : (unsigned long long)QCLAIM;
+        if (atomicCAS(a.q.head + b, h, h + k) == h) {
+          unsigned long long* seq = a.q.seq + (unsigned long long)b * cap;
+          for (unsigned long long j = 0; j < k; j++) {
+            const unsigned long long pos = h + j, slot = pos & a.q.mask;
+            const long long tt0 = gtimer_ns();
+            bool ok = true;
+            while (ld_volatile(seq + slot) != pos + 1) {
+              if (gtimer_ns() - tt0 > a.timeout_ns) {
+                atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
+                atomicExch(a.abort_flag, 1);
+                ok = false;
+                break;
+              }
+              __nanosleep(32);
+            }
+            if (!ok) break;
+            items_out[got++] = ld_volatile(a.q.items + (unsigned long long)b * cap + slot);
+            __threadfence();
+            atomicExch(seq + slot, pos + cap);
+          }
+        }
       }
-      __nanosleep(32);
     }
-    *item = ld_volatile(a.q.items + slot);
-    __threadfence();
-    atomicExch(a.q.seq + slot, h + a.q.mask + 1);
-    return true;
+    got = __shfl_sync(0xffffffffu, got, 0);
+    if (got) {
+      for (int j = 0; j < QCLAIM; j++) items_out[j] = __shfl_sync(0xffffffffu, items_out[j], 0);
+      return got;
+    }
+    if (*(volatile int*)a.abort_flag) return 0;
+    if (lane == 0) __nanosleep(20 + (threadIdx.x * 7 + attempt * 13) % 200);
+    __syncwarp();
   }
+  return 0;
+}
+
+// Bucket of a trigger time; a nearly full bucket spills into the next one (ordering degrades
+// gracefully instead of a producer waiting on a full ring).
+__device__ __forceinline__ int bucket_of(const SolveArgs& a, const CoarseProblem& P, double prio) {
+  const double x = prio * P.tinv;
+  int b = (!(x < (double)(QBUCKETS - 1))) ? QBUCKETS - 1 : (x > 0.0 ? (int)x : 0);
+  const unsigned long long lim = (a.q.mask + 1) - 4096;
+  while (b < QBUCKETS - 1 && ld_volatile(a.q.tail + b) - ld_volatile(a.q.head + b) >= lim) b++;
+  return b;
 }
 
 // Tile states: 0 idle, 1 queued, 2 being processed, 3 being processed and changed again
@@ -72,16 +115,24 @@ __device__ bool q_pop(const SolveArgs& a, unsigned long long* item) {
 // processed by two CTAs at once, so a write-back can never overwrite newer values.
 constexpr int TS_IDLE = 0, TS_QUEUED = 1, TS_BUSY = 2, TS_BUSY_DIRTY = 3;
 
-__device__ void enqueue_tile(const SolveArgs& a, int prob, long long tile, uint32_t faces) {
+__device__ __forceinline__ unsigned long long tile_item(int prob, long long tile) {
+  return ((unsigned long long)prob << 40) | (unsigned long long)tile;
+}
+
+// Marks faces of a tile dirty with trigger time prio and queues it unless it is queued
+// already or its current processor will re-queue it.
+__device__ void enqueue_tile(const SolveArgs& a, int prob, long long tile, uint32_t faces, double prio) {
   const long long gt = a.probs[prob].tbase + tile;
   atomicOr(a.tile_faces + gt, faces);
+  atomicMin(a.tile_prio + gt, (unsigned long long)__double_as_longlong(prio));
   int s = *(volatile int*)(a.tile_flag + gt);
   for (int it = 0; it < 64; it++) {
     if (s == TS_IDLE) {
       const int o = atomicCAS(a.tile_flag + gt, TS_IDLE, TS_QUEUED);
       if (o == TS_IDLE) {
         atomicAdd(a.pending, 1);
-        q_push(a, ((unsigned long long)prob << 40) | (unsigned long long)tile);
+        const double pr = __longlong_as_double((long long)ld_volatile(a.tile_prio + gt));
+        q_push(a, bucket_of(a, a.probs[prob], pr), tile_item(prob, tile));
         return;
       }
       s = o;
@@ -107,20 +158,22 @@ __device__ void finish_tile(const SolveArgs& a, int prob, long long tile) {
   }
   // TS_BUSY_DIRTY: stays counted in pending, goes back to the queue
   atomicExch(a.tile_flag + gt, TS_QUEUED);
-  q_push(a, ((unsigned long long)prob << 40) | (unsigned long long)tile);
+  const double pr = __longlong_as_double((long long)ld_volatile(a.tile_prio + gt));
+  q_push(a, bucket_of(a, a.probs[prob], pr), tile_item(prob, tile));
 }
 
 // ------------------------------------------------------------------ tile shapes --
 template <int ND> struct TileCfg;
 template <> struct TileCfg<3> {
-  static constexpr int TX = 8, TY = 8, TZ = 8, H = 2;
+  static constexpr int TX = 4, TY = 4, TZ = 4, H = 2;
   static constexpr int HX = TX + 2 * H, HY = TY + 2 * H, HZ = TZ + 2 * H;
 };
 template <> struct TileCfg<2> {
-  static constexpr int TX = 32, TY = 16, TZ = 1, H = 2;
+  static constexpr int TX = 8, TY = 8, TZ = 1, H = 2;
   static constexpr int HX = TX + 2 * H, HY = TY + 2 * H, HZ = 1;
 };
-constexpr int SOLVE_THREADS = 256;
+constexpr int SOLVE_THREADS = 256;  // 8 warps, one tile per warp
+constexpr int SOLVE_WARPS = SOLVE_THREADS / 32;
 
 // ----------------------------------------------------------------------- init --
 __global__ void coarse_init_kernel(const CoarseProblem* probs, int nprob, long long N) {
@@ -135,17 +188,21 @@ __global__ void coarse_init_kernel(const CoarseProblem* probs, int nprob, long l
 }
 
 __global__ void queue_init_kernel(SolveArgs a) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < (long long)a.q.mask + 1;
+  const long long cap = (long long)a.q.mask + 1;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < cap * QBUCKETS;
        q += (long long)gridDim.x * blockDim.x)
-    a.q.seq[q] = (unsigned long long)q;
+    a.q.seq[q] = (unsigned long long)(q % cap);
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.ntiles;
        q += (long long)gridDim.x * blockDim.x) {
     a.tile_faces[q] = 0;
     a.tile_flag[q] = 0;
+    a.tile_prio[q] = (unsigned long long)__double_as_longlong(EIK_INF);
+  }
+  if (blockIdx.x == 0 && threadIdx.x < QBUCKETS) {
+    a.q.head[threadIdx.x] = 0;
+    a.q.tail[threadIdx.x] = 0;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *a.q.head = 0;
-    *a.q.tail = 0;
     *a.pending = 0;
     *a.activations = 0;
     *a.node_evals = 0;
@@ -181,59 +238,140 @@ __global__ void seed_kernel(SolveArgs a, ForwardBatch fb) {
     const int j = (int)((l / P.g.n[0]) % P.g.n[1]);
     const int k = (int)(l / ((long long)P.g.n[0] * P.g.n[1]));
     const int c[3] = {i, j, k};
-    enqueue_tile(a, s, tile_of<ND>(P, i, j, k), FACES_ALL);
+    const double pr = fb.seed_tt[(size_t)s * fb.seedcap + q];
+    enqueue_tile(a, s, tile_of<ND>(P, i, j, k), FACES_ALL, pr);
     for (int ax = 0; ax < ND; ax++)
       for (int d = -2; d <= 2; d += 4) {
         int p[3] = {c[0], c[1], c[2]};
         p[ax] += d;
         if (p[ax] < 0 || p[ax] >= P.g.n[ax]) continue;
-        enqueue_tile(a, s, tile_of<ND>(P, p[0], p[1], p[2]), FACES_ALL);
+        enqueue_tile(a, s, tile_of<ND>(P, p[0], p[1], p[2]), FACES_ALL, pr);
       }
   }
 }
 
 // ------------------------------------------------------------------ tile solve --
+// One warp owns one tile at a time (its own shared-memory slice, warp-level syncs only),
+// so an SM keeps many independent tiles in flight and hides the FP64 latency of the
+// update; CTAs only group warps for occupancy.
 template <int ND>
 struct TileSmem {
   using C = TileCfg<ND>;
   static constexpr int TN = C::TX * C::TY * C::TZ;
   static constexpr int HN = C::HX * C::HY * C::HZ;
   double t[HN];
-  double L[HN];
+  double L[HN];       // key level of special nodes
   double slow[TN];
-  uint8_t fl[HN];  // bit0 special, bits1..7 depth
+  uint8_t fl[HN];     // bit0 special key, bits 1..4 depth
   uint8_t code[TN];
-  uint8_t act[TN];
-  uint8_t nxt[TN];
-  uint8_t dirty[TN];
+  uint8_t act[TN];    // to be evaluated (plain stores of 1 from any lane)
+  uint8_t dirty[TN];  // changed, to be written back
+  int16_t list[TN];
 };
 
 template <int ND>
-__device__ __forceinline__ Key smem_key(const TileSmem<ND>& S, int h) {
-  const uint8_t f = S.fl[h];
-  if (f & 1) {
-    const double L = S.L[h];
-    if (L == -EIK_INF) return key_source();
-    return Key{L, (int)(f >> 1), S.t[h]};
-  }
-  return key_normal(S.t[h]);
+__device__ __forceinline__ int hidx(int x, int y, int z) {
+  using C = TileCfg<ND>;
+  return (x + C::H) + C::HX * ((y + C::H) + C::HY * (ND == 3 ? z + C::H : 0));
 }
 
 template <int ND>
-__device__ void process_tile(const SolveArgs& a, TileSmem<ND>& S, int prob, long long tile, uint32_t faces,
-                             int* sh_faces_out, int* sh_unconv) {
+__device__ __forceinline__ void smem_keyLd(const TileSmem<ND>& S, int h, double* L, int* d) {
+  const uint8_t f = S.fl[h];
+  if (f & 1) {
+    *L = S.L[h];
+    *d = f >> 1;
+  } else {
+    *L = S.t[h];
+    *d = 0;
+  }
+}
+
+// Smallest traveltime among the in-grid immediate neighbours of tile node li.
+template <int ND>
+__device__ __forceinline__ double node_potential(const TileSmem<ND>& S, const GridDesc& g, int ox, int oy,
+                                                 int oz, int li) {
+  using C = TileCfg<ND>;
+  const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
+  const int c[3] = {ox + x, oy + y, oz + z};
+  const int hc[3] = {x, y, z};
+  double pm = EIK_INF;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int sh = -1; sh <= 1; sh += 2) {
+      if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
+      int q[3] = {hc[0], hc[1], hc[2]};
+      q[ax] += sh;
+      pm = fmin(pm, S.t[hidx<ND>(q[0], q[1], q[2])]);
+    }
+  return pm;
+}
+
+template <int ND>
+__device__ __forceinline__ double eval_node(const TileSmem<ND>& S, const GridDesc& g, int ox, int oy, int oz,
+                                            int li, int8_t* cd, Key* kk, bool* neg) {
+  using C = TileCfg<ND>;
+  const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
+  const int c[3] = {ox + x, oy + y, oz + z};
+  const int hc[3] = {x, y, z};
+  Nbhd nb;
+  nb_clear(nb);
+  node_dh(g, c[0], nb.dh);
+  nb.slow = S.slow[li];
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int l = 0; l < 2; l++) {
+      const int sh = l == 0 ? 1 : -1;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      if (p[ax] < 0 || p[ax] >= g.n[ax]) continue;
+      int q[3] = {hc[0], hc[1], hc[2]};
+      q[ax] += sh;
+      const int h1 = hidx<ND>(q[0], q[1], q[2]);
+      double L;
+      int d;
+      smem_keyLd<ND>(S, h1, &L, &d);
+      nb_put1(nb, ax, l, S.t[h1], L, d);
+      bool ok = true;
+#pragma unroll
+      for (int dd = 0; dd < ND; dd++)
+        if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
+      if (ok) {
+        q[ax] += sh;
+        const int h2 = hidx<ND>(q[0], q[1], q[2]);
+        smem_keyLd<ND>(S, h2, &L, &d);
+        nb_put2(nb, ax, l, S.t[h2], L, d);
+      }
+    }
+  return prefix_rule<ND>(nb, cd, kk, neg);
+}
+
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Processes one tile with the 32 lanes of the calling warp. Returns the dirty-face mask
+// (bit 6: not converged within the pass limit) and the smallest changed face traveltime.
+template <int ND>
+__device__ int process_tile(const SolveArgs& a, TileSmem<ND>& S, int prob, long long tile, uint32_t faces,
+                            double* fmin_out) {
   using C = TileCfg<ND>;
   constexpr int TN = TileSmem<ND>::TN, HN = TileSmem<ND>::HN;
+  constexpr int NPT = (TN + 31) / 32;
   const CoarseProblem& P = a.probs[prob];
   const GridDesc& g = P.g;
   const int tx = (int)(tile % P.nt[0]);
   const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
   const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
   const int ox = tx * C::TX, oy = ty * C::TY, oz = tz * C::TZ;
-  const int tid = threadIdx.x;
+  const int lane = threadIdx.x & 31;
 
   // ---- stage tile + halo
-  for (int h = tid; h < HN; h += SOLVE_THREADS) {
+  for (int h = lane; h < HN; h += 32) {
     const int hx = h % C::HX, hy = (h / C::HX) % C::HY, hz = h / (C::HX * C::HY);
     const int gx = ox + hx - C::H, gy = oy + hy - C::H, gz = (ND == 3) ? oz + hz - C::H : 0;
     double tv = EIK_INF, Lv = 0.0;
@@ -258,117 +396,109 @@ __device__ void process_tile(const SolveArgs& a, TileSmem<ND>& S, int prob, long
     S.L[h] = Lv;
     S.fl[h] = f;
   }
-  if (tid == 0) *sh_faces_out = 0;
-  __syncthreads();
-  // ---- initial active set from the dirty faces
-  for (int li = tid; li < TN; li += SOLVE_THREADS) {
+  __syncwarp();
+  // ---- initial active set from the dirty faces (source points are never updated)
+#pragma unroll
+  for (int r = 0; r < NPT; r++) {
+    const int li = lane + 32 * r;
+    if (li >= TN) continue;
     const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-    const int gx = ox + x, gy = oy + y, gz = oz + z;
     bool act = (faces & FACES_ALL) != 0;
     act = act || ((faces & 1) && x < 2) || ((faces & 2) && x >= C::TX - 2) || ((faces & 4) && y < 2) ||
           ((faces & 8) && y >= C::TY - 2) || ((faces & 16) && z < 2) || ((faces & 32) && z >= C::TZ - 2);
-    const int h = (x + C::H) + C::HX * ((y + C::H) + C::HY * (ND == 3 ? z + C::H : 0));
+    const int h = hidx<ND>(x, y, z);
     const bool src = (S.fl[h] & 1) && S.L[h] == -EIK_INF;
-    const bool inside = gx < g.n[0] && gy < g.n[1] && gz < g.n[2];
+    const bool inside = ox + x < g.n[0] && oy + y < g.n[1] && oz + z < g.n[2];
     S.act[li] = (act && !src && inside) ? 1 : 0;
-    S.nxt[li] = 0;
     S.dirty[li] = 0;
   }
-  __syncthreads();
+  double hmin = g.spac[0];
+  if (!is_cart(g)) {
+    double dh[3];
+    node_dh(g, 0, dh);
+    hmin = fmin(dh[0], dh[1]);
+    if (ND == 3) hmin = fmin(hmin, dh[2]);
+  }
+  const double gate = a.gate * hmin;
+  __syncwarp();
 
-  constexpr int NPT = (TN + SOLVE_THREADS - 1) / SOLVE_THREADS;
+  int fm = 0;
+  double fmin_changed = EIK_INF;
   int pass = 0;
   unsigned long long evals = 0;
-  bool any = true;
-  while (any) {
+  bool unconv = false;
+  for (;;) {
+    // ---- front of the active nodes, gated evaluation list
+    double pot[NPT];
+    double mypot = EIK_INF;
+#pragma unroll
+    for (int r = 0; r < NPT; r++) {
+      const int li = lane + 32 * r;
+      pot[r] = EIK_INF;
+      if (li >= TN || !S.act[li]) continue;
+      pot[r] = node_potential<ND>(S, g, ox, oy, oz, li);
+      if (!(pot[r] < EIK_INF)) S.act[li] = 0;  // no reached neighbour: nothing to compute
+      mypot = fmin(mypot, pot[r]);
+    }
+    const double front = warp_min(mypot);
+    if (!(front < EIK_INF)) break;
+    int nlist = 0;
+#pragma unroll
+    for (int r = 0; r < NPT; r++) {
+      const int li = lane + 32 * r;
+      const bool sel = li < TN && S.act[li] && pot[r] <= front + gate * S.slow[li];
+      const unsigned m = __ballot_sync(0xffffffffu, sel);
+      if (sel) {
+        S.list[nlist + __popc(m & ((1u << lane) - 1u))] = (int16_t)li;
+        S.act[li] = 0;
+      }
+      nlist += __popc(m);
+    }
+    __syncwarp();
+    // ---- evaluate
     double nv[NPT];
     Key nk[NPT];
     uint8_t nc[NPT];
-    bool ch[NPT];
+    int nli[NPT];
 #pragma unroll
     for (int r = 0; r < NPT; r++) {
-      ch[r] = false;
-      const int li = tid + r * SOLVE_THREADS;
-      if (li >= TN || !S.act[li]) continue;
-      const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-      const int c[3] = {ox + x, oy + y, oz + z};
-      const int hc[3] = {x + C::H, y + C::H, ND == 3 ? z + C::H : 0};
-      Nbhd nb;
-      node_dh(g, c[0], nb.dh);
-      nb.slow = S.slow[li];
-#pragma unroll
-      for (int ax = 0; ax < 3; ax++)
-#pragma unroll
-        for (int l = 0; l < 2; l++) {
-          nb.in1[ax][l] = false;
-          nb.ok2[ax][l] = false;
-          nb.t1[ax][l] = EIK_INF;
-          nb.t2[ax][l] = EIK_INF;
-          nb.k1[ax][l] = key_unreached();
-          nb.k2[ax][l] = key_unreached();
-        }
-#pragma unroll
-      for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-        for (int l = 0; l < 2; l++) {
-          const int sh = l == 0 ? 1 : -1;
-          int p[3] = {c[0], c[1], c[2]};
-          p[ax] += sh;
-          if (p[ax] < 0 || p[ax] >= g.n[ax]) continue;
-          nb.in1[ax][l] = true;
-          int hp[3] = {hc[0], hc[1], hc[2]};
-          hp[ax] += sh;
-          const int h1 = hp[0] + C::HX * (hp[1] + C::HY * hp[2]);
-          nb.t1[ax][l] = S.t[h1];
-          nb.k1[ax][l] = smem_key<ND>(S, h1);
-          bool ok = true;
-#pragma unroll
-          for (int d = 0; d < ND; d++)
-            if (p[d] < 1 || p[d] > g.n[d] - 2) ok = false;
-          nb.ok2[ax][l] = ok;
-          if (ok) {
-            hp[ax] += sh;
-            const int h2 = hp[0] + C::HX * (hp[1] + C::HY * hp[2]);
-            nb.t2[ax][l] = S.t[h2];
-            nb.k2[ax][l] = smem_key<ND>(S, h2);
-          }
-        }
+      const int e = lane + 32 * r;
+      nli[r] = -1;
+      if (e >= nlist) continue;
+      const int li = S.list[e];
       int8_t cd[3] = {0, 0, 0};
-      Key kk;
       bool neg = false;
-      const double v = prefix_rule<ND>(nb, cd, &kk, &neg);
+      nv[r] = eval_node<ND>(S, g, ox, oy, oz, li, cd, &nk[r], &neg);
+      nc[r] = pack_codes(cd, ND);
+      nli[r] = li;
       evals++;
-      const int hm = hc[0] + C::HX * (hc[1] + C::HY * hc[2]);
-      const Key old = smem_key<ND>(S, hm);
-      const double ot = S.t[hm];
-      const uint8_t pc = pack_codes(cd, ND);
-      const bool same_t = (v == ot) || (isinf(v) && isinf(ot));
-      nv[r] = v;
-      nk[r] = kk;
-      nc[r] = pc;
-      ch[r] = !(same_t && key_eq(kk, old)) || pc != S.code[li];
     }
-    __syncthreads();
-    bool anyc = false;
+    __syncwarp();
+    // ---- apply
 #pragma unroll
     for (int r = 0; r < NPT; r++) {
-      if (!ch[r]) continue;
-      const int li = tid + r * SOLVE_THREADS;
+      const int li = nli[r];
+      if (li < 0) continue;
       const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-      const int hc[3] = {x + C::H, y + C::H, ND == 3 ? z + C::H : 0};
-      const int hm = hc[0] + C::HX * (hc[1] + C::HY * hc[2]);
-      const bool tkchange = !(((nv[r] == S.t[hm]) || (isinf(nv[r]) && isinf(S.t[hm]))) &&
-                              key_eq(nk[r], smem_key<ND>(S, hm)));
-      S.t[hm] = nv[r];
-      const bool special = !(nk[r].L == nk[r].t && nk[r].d == 0);
-      S.fl[hm] = special ? (uint8_t)(1 | (nk[r].d << 1)) : (uint8_t)0;
-      S.L[hm] = special ? nk[r].L : 0.0;
+      const int hm = hidx<ND>(x, y, z);
+      double Lo;
+      int dold;
+      smem_keyLd<ND>(S, hm, &Lo, &dold);
+      const double ot = S.t[hm];
+      const Key old = Key{Lo, dold, ot};
+      const bool same_t = (nv[r] == ot) || (isinf(nv[r]) && isinf(ot));
+      const bool tkchange = !(same_t && key_eq(nk[r], old));
+      if (!tkchange && nc[r] == S.code[li]) continue;
       S.code[li] = nc[r];
       S.dirty[li] = 1;
       if (!tkchange) continue;
-      anyc = true;
+      S.t[hm] = nv[r];
+      const bool special = !(nk[r].L == nv[r] && nk[r].d == 0);
+      S.fl[hm] = special ? (uint8_t)(1 | (nk[r].d << 1)) : (uint8_t)0;
+      S.L[hm] = special ? nk[r].L : 0.0;
       const int xyz[3] = {x, y, z};
       const int T3[3] = {C::TX, C::TY, C::TZ};
+      const int o3[3] = {ox, oy, oz};
 #pragma unroll
       for (int ax = 0; ax < ND; ax++)
 #pragma unroll
@@ -376,44 +506,45 @@ __device__ void process_tile(const SolveArgs& a, TileSmem<ND>& S, int prob, long
           if (d == 0) continue;
           int q[3] = {xyz[0], xyz[1], xyz[2]};
           q[ax] += d;
-          if (q[ax] < 0 || q[ax] >= T3[ax]) continue;
+          if (q[ax] < 0 || q[ax] >= T3[ax] || o3[ax] + q[ax] >= g.n[ax]) continue;
           const int lq = q[0] + C::TX * (q[1] + C::TY * q[2]);
-          S.nxt[lq] = 1;
+          const int hq = hidx<ND>(q[0], q[1], q[2]);
+          const bool src = (S.fl[hq] & 1) && S.L[hq] == -EIK_INF;
+          if (!src) S.act[lq] = 1;
         }
-      int fm = 0;
-      if (x < 2) fm |= 1;
-      if (x >= C::TX - 2) fm |= 2;
-      if (y < 2) fm |= 4;
-      if (y >= C::TY - 2) fm |= 8;
-      if (ND == 3 && z < 2) fm |= 16;
-      if (ND == 3 && z >= C::TZ - 2) fm |= 32;
-      if (fm) atomicOr(sh_faces_out, fm);
+      int f = 0;
+      if (x < 2) f |= 1;
+      if (x >= C::TX - 2) f |= 2;
+      if (y < 2) f |= 4;
+      if (y >= C::TY - 2) f |= 8;
+      if (ND == 3 && z < 2) f |= 16;
+      if (ND == 3 && z >= C::TZ - 2) f |= 32;
+      if (f) {
+        fm |= f;
+        fmin_changed = fmin(fmin_changed, nv[r]);
+      }
     }
-    __syncthreads();
-    bool anyact = false;
-    for (int li = tid; li < TN; li += SOLVE_THREADS) {
-      const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-      const int h = (x + C::H) + C::HX * ((y + C::H) + C::HY * (ND == 3 ? z + C::H : 0));
-      const bool src = (S.fl[h] & 1) && S.L[h] == -EIK_INF;
-      const bool inside = ox + x < g.n[0] && oy + y < g.n[1] && oz + z < g.n[2];
-      const uint8_t a2 = (S.nxt[li] && !src && inside) ? 1 : 0;
-      S.act[li] = a2;
-      S.nxt[li] = 0;
-      anyact = anyact || a2;
-    }
-    (void)anyc;
+    __syncwarp();
     pass++;
-    any = __syncthreads_or(anyact) != 0;
-    if (any && pass >= a.max_passes) {
-      if (tid == 0) *sh_unconv = 1;
+    bool anyact = false;
+#pragma unroll
+    for (int r = 0; r < NPT; r++) {
+      const int li = lane + 32 * r;
+      anyact = anyact || (li < TN && S.act[li]);
+    }
+    if (!__any_sync(0xffffffffu, anyact)) break;
+    if (pass >= a.max_passes) {
+      unconv = true;
       break;
     }
   }
   // ---- write back
-  for (int li = tid; li < TN; li += SOLVE_THREADS) {
-    if (!S.dirty[li]) continue;
+#pragma unroll
+  for (int r = 0; r < NPT; r++) {
+    const int li = lane + 32 * r;
+    if (li >= TN || !S.dirty[li]) continue;
     const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-    const int h = (x + C::H) + C::HX * ((y + C::H) + C::HY * (ND == 3 ? z + C::H : 0));
+    const int h = hidx<ND>(x, y, z);
     const long long l = lin3(g, ox + x, oy + y, oz + z);
     P.t[l] = S.t[h];
     const bool special = S.fl[h] & 1;
@@ -423,87 +554,90 @@ __device__ void process_tile(const SolveArgs& a, TileSmem<ND>& S, int prob, long
       P.kd[l] = (uint8_t)(S.fl[h] >> 1);
     }
   }
-  if (evals) atomicAdd(a.node_evals, evals);
+  // reduce face mask and trigger time over the warp
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) fm |= __shfl_xor_sync(0xffffffffu, fm, o);
+  *fmin_out = warp_min(fmin_changed);
+  unsigned long long ev = evals;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
+  if (lane == 0 && ev) atomicAdd(a.node_evals, ev);
+  return fm | (unconv ? 64 : 0);
 }
 
 template <int ND>
-__global__ void __launch_bounds__(SOLVE_THREADS) coarse_solve_kernel(SolveArgs a) {
-  using C = TileCfg<ND>;
-  __shared__ TileSmem<ND> S;
-  __shared__ unsigned long long sh_item;
-  __shared__ int sh_state;  // 0 work, 1 wait, 2 exit
-  __shared__ uint32_t sh_faces_in;
-  __shared__ int sh_faces_out, sh_unconv;
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_solve_kernel(SolveArgs a) {
+  extern __shared__ __align__(16) unsigned char solve_smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  TileSmem<ND>& S = reinterpret_cast<TileSmem<ND>*>(solve_smem)[warp];
   long long idle_since = -1;
   for (;;) {
-    if (threadIdx.x == 0) {
-      unsigned long long it;
-      if (*(volatile int*)a.abort_flag) {
-        sh_state = 2;
-      } else if (q_pop(a, &it)) {
-        sh_state = 0;
-        sh_item = it;
-        const int prob = (int)(it >> 40);
-        const long long tile = (long long)(it & ((1ull << 40) - 1));
-        const long long gt = a.probs[prob].tbase + tile;
-        atomicExch(a.tile_flag + gt, TS_BUSY);
-        sh_faces_in = atomicExch(a.tile_faces + gt, 0u);
-        __threadfence();
-        const unsigned long long na = atomicAdd(a.activations, 1ull);
-        if (na > a.max_activations) {
-          atomicOr(a.err, ERRB_NOT_CONVERGED);
-          atomicExch(a.abort_flag, 1);
-        }
-        sh_unconv = 0;
-        idle_since = -1;
-      } else if (*(volatile int*)a.pending == 0) {
-        sh_state = 2;
-      } else {
-        sh_state = 1;
+    int ab = (lane == 0) ? *(volatile int*)a.abort_flag : 0;
+    if (__shfl_sync(0xffffffffu, ab, 0)) break;
+    unsigned long long its[QCLAIM] = {0, 0, 0, 0};
+    const int ngot = q_pop_warp(a, its);
+    if (!ngot) {
+      int done = (lane == 0) ? (*(volatile int*)a.pending == 0) : 0;
+      if (__shfl_sync(0xffffffffu, done, 0)) break;
+      if (lane == 0) {
         const long long now = gtimer_ns();
         if (idle_since < 0) idle_since = now;
         if (now - idle_since > a.timeout_ns) {
           atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
           atomicExch(a.abort_flag, 1);
         }
+        __nanosleep(200);
       }
-    }
-    __syncthreads();
-    const int state = sh_state;
-    if (state == 2) break;
-    if (state == 1) {
-      if (threadIdx.x == 0) __nanosleep(256);
-      __syncthreads();
+      __syncwarp();
       continue;
     }
-    const int prob = (int)(sh_item >> 40);
-    const long long tile = (long long)(sh_item & ((1ull << 40) - 1));
-    process_tile<ND>(a, S, prob, tile, sh_faces_in, &sh_faces_out, &sh_unconv);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const CoarseProblem& P = a.probs[prob];
-      const int tx = (int)(tile % P.nt[0]);
-      const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
-      const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
-      const int fm = sh_faces_out;
-      auto nbt = [&](int x, int y, int z) { return (long long)x + (long long)P.nt[0] * (y + (long long)P.nt[1] * z); };
-      if ((fm & 1) && tx > 0) enqueue_tile(a, prob, nbt(tx - 1, ty, tz), 2u);
-      if ((fm & 2) && tx + 1 < P.nt[0]) enqueue_tile(a, prob, nbt(tx + 1, ty, tz), 1u);
-      if ((fm & 4) && ty > 0) enqueue_tile(a, prob, nbt(tx, ty - 1, tz), 8u);
-      if ((fm & 8) && ty + 1 < P.nt[1]) enqueue_tile(a, prob, nbt(tx, ty + 1, tz), 4u);
-      if (ND == 3) {
-        if ((fm & 16) && tz > 0) enqueue_tile(a, prob, nbt(tx, ty, tz - 1), 32u);
-        if ((fm & 32) && tz + 1 < P.nt[2]) enqueue_tile(a, prob, nbt(tx, ty, tz + 1), 16u);
+    idle_since = -1;
+    for (int j = 0; j < ngot; j++) {
+      const unsigned long long it = its[j];
+      const int prob = (int)(it >> 40);
+      const long long tile = (long long)(it & ((1ull << 40) - 1));
+      const long long gt = a.probs[prob].tbase + tile;
+      uint32_t faces = 0;
+      if (lane == 0) {
+        atomicExch(a.tile_flag + gt, TS_BUSY);
+        faces = atomicExch(a.tile_faces + gt, 0u);
+        atomicExch(a.tile_prio + gt, (unsigned long long)__double_as_longlong(EIK_INF));
+        __threadfence();
+        const unsigned long long na = atomicAdd(a.activations, 1ull);
+        if (na > a.max_activations) {
+          atomicOr(a.err, ERRB_NOT_CONVERGED);
+          atomicExch(a.abort_flag, 1);
+        }
       }
-      if (sh_unconv) {
-        atomicOr(a.tile_faces + P.tbase + tile, FACES_ALL);
-        atomicExch(a.tile_flag + P.tbase + tile, TS_BUSY_DIRTY);
-      }
+      faces = __shfl_sync(0xffffffffu, faces, 0);
+      double pr;
+      const int fm = process_tile<ND>(a, S, prob, tile, faces, &pr);
       __threadfence();
-      finish_tile(a, prob, tile);
+      __syncwarp();
+      if (lane == 0) {
+        const CoarseProblem& P = a.probs[prob];
+        const int tx = (int)(tile % P.nt[0]);
+        const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
+        const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
+        auto nbt = [&](int x, int y, int z) { return (long long)x + (long long)P.nt[0] * (y + (long long)P.nt[1] * z); };
+        if ((fm & 1) && tx > 0) enqueue_tile(a, prob, nbt(tx - 1, ty, tz), 2u, pr);
+        if ((fm & 2) && tx + 1 < P.nt[0]) enqueue_tile(a, prob, nbt(tx + 1, ty, tz), 1u, pr);
+        if ((fm & 4) && ty > 0) enqueue_tile(a, prob, nbt(tx, ty - 1, tz), 8u, pr);
+        if ((fm & 8) && ty + 1 < P.nt[1]) enqueue_tile(a, prob, nbt(tx, ty + 1, tz), 4u, pr);
+        if (ND == 3) {
+          if ((fm & 16) && tz > 0) enqueue_tile(a, prob, nbt(tx, ty, tz - 1), 32u, pr);
+          if ((fm & 32) && tz + 1 < P.nt[2]) enqueue_tile(a, prob, nbt(tx, ty, tz + 1), 16u, pr);
+        }
+        if (fm & 64) {
+          atomicOr(a.tile_faces + gt, FACES_ALL);
+          atomicMin(a.tile_prio + gt, (unsigned long long)__double_as_longlong(pr));
+          atomicExch(a.tile_flag + gt, TS_BUSY_DIRTY);
+        }
+        __threadfence();
+        finish_tile(a, prob, tile);
+      }
+      __syncwarp();
     }
-    __syncthreads();
   }
 }
 
@@ -564,17 +698,23 @@ void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs
   else seed_kernel<2><<<nprob, 128, 0, st>>>(sa, fb);
 }
 
-void launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st) {
-  int per = 1;
-  if (sa.nd == 3) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_solve_kernel<3>, SOLVE_THREADS, 0);
-    per = per < 1 ? 1 : per;
-    coarse_solve_kernel<3><<<nsm * per, SOLVE_THREADS, 0, st>>>(sa);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_solve_kernel<2>, SOLVE_THREADS, 0);
-    per = per < 1 ? 1 : per;
-    coarse_solve_kernel<2><<<nsm * per, SOLVE_THREADS, 0, st>>>(sa);
+template <int ND>
+static void launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st) {
+  const size_t sm = sizeof(TileSmem<ND>) * SOLVE_WARPS;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(coarse_solve_kernel<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    attr = true;
   }
+  int per = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_solve_kernel<ND>, SOLVE_THREADS, sm);
+  per = per < 1 ? 1 : per;
+  coarse_solve_kernel<ND><<<nsm * per, SOLVE_THREADS, sm, st>>>(sa);
+}
+
+void launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st) {
+  if (sa.nd == 3) launch_solve_nd<3>(sa, nsm, st);
+  else launch_solve_nd<2>(sa, nsm, st);
 }
 
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,

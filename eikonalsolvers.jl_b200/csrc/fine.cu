@@ -80,44 +80,28 @@ __device__ __forceinline__ double fine_update(const GridDesc& gf, const double* 
                                               double slow, int i, int j, int k, int8_t* codes,
                                               bool* neg) {
   Nbhd nb;
+  nb_clear(nb);
   const int c[3] = {i, j, k};
   node_dh(gf, i, nb.dh);
   nb.slow = slow;
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-#pragma unroll
-    for (int l = 0; l < 2; l++) {
-      nb.in1[a][l] = false;
-      nb.ok2[a][l] = false;
-      nb.t1[a][l] = EIK_INF;
-      nb.t2[a][l] = EIK_INF;
-      nb.k1[a][l] = key_unreached();
-      nb.k2[a][l] = key_unreached();
-    }
   for (int a = 0; a < gf.nd; a++)
     for (int l = 0; l < 2; l++) {
       const int sh = l == 0 ? 1 : -1;
       int p[3] = {c[0], c[1], c[2]};
       p[a] += sh;
       if (p[a] < 0 || p[a] >= gf.n[a]) continue;
-      nb.in1[a][l] = true;
       const long long pl = lin3(gf, p[0], p[1], p[2]);
-      if (st[pl] == 2) {
-        nb.t1[a][l] = tt[pl];
-        nb.k1[a][l] = key_source();
-      }
+      if (st[pl] == 2) nb_put1(nb, a, l, tt[pl], -EIK_INF, 0);
+      else nb_put1(nb, a, l, EIK_INF, EIK_INF, 0);
       bool ok = true;
       for (int d = 0; d < gf.nd; d++)
         if (p[d] < 1 || p[d] > gf.n[d] - 2) ok = false;
-      nb.ok2[a][l] = ok;
       if (ok) {
         int q[3] = {p[0], p[1], p[2]};
         q[a] += sh;
         const long long ql = lin3(gf, q[0], q[1], q[2]);
-        if (st[ql] == 2) {
-          nb.t2[a][l] = tt[ql];
-          nb.k2[a][l] = key_source();
-        }
+        if (st[ql] == 2) nb_put2(nb, a, l, tt[ql], -EIK_INF, 0);
+        else nb_put2(nb, a, l, EIK_INF, EIK_INF, 0);
       }
     }
   const Key T = key_normal(0.0);

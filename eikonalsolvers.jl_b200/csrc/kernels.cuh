@@ -63,14 +63,19 @@ struct CoarseProblem {
   int32_t nt[3];   // tiles per axis
   int32_t pad;
   long long tbase; // first global tile id of this problem
+  double tinv;     // QBUCKETS / (time scale of this problem): trigger time -> bucket
 };
 
-// Bounded multi-producer/multi-consumer ring of tile ids (Vyukov's sequence scheme).
+// Bucketed priority queue of tile ids: QBUCKETS bounded multi-producer/multi-consumer
+// rings (Vyukov's sequence scheme), bucket = trigger time of the tile scaled by its
+// problem's time scale. Consumers take from the lowest non-empty bucket, so tiles are
+// processed roughly in the order the fast-marching front reaches them.
+constexpr int QBUCKETS = 64;
 struct TileQueue {
-  unsigned long long* items;
-  unsigned long long* seq;
-  unsigned long long* head;
-  unsigned long long* tail;
+  unsigned long long* items;  // QBUCKETS x (mask+1)
+  unsigned long long* seq;    // QBUCKETS x (mask+1)
+  unsigned long long* head;   // QBUCKETS
+  unsigned long long* tail;   // QBUCKETS
   unsigned long long mask;
 };
 
@@ -80,6 +85,7 @@ struct SolveArgs {
   int32_t nd;
   long long ntiles;            // total tiles over all problems
   uint32_t* tile_faces;        // pending dirty faces per tile (bit 6: whole tile)
+  unsigned long long* tile_prio;  // smallest pending trigger time per tile (double bits)
   int32_t* tile_flag;          // 1 while queued
   TileQueue q;
   int32_t* pending;            // tiles queued or being processed
@@ -89,6 +95,7 @@ struct SolveArgs {
   uint32_t* err;
   int32_t* abort_flag;
   int32_t max_passes;
+  double gate;                 // in-tile front gate, in units of (node spacing x slowness)
   long long timeout_ns;
 };
 

@@ -31,6 +31,7 @@ struct Model {
   long long N = 0;
   double* vel = nullptr;   // device
   double* slow = nullptr;  // device, 1.0/vel
+  double tscale = 1.0;     // grid diagonal x mean slowness (tile scheduling only)
 };
 
 // Device results of the forward stage of one call.

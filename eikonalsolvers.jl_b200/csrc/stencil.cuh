@@ -45,7 +45,7 @@ namespace eik {
 // key (L, d, .), produced a value v <= L is accepted right after that trigger although v is
 // below the current front (the reference overwrites band values, BinHeaps.jl:394-430, and
 // takes no causality check, eikforward2D.jl:425-430): its key is (L, d+1, v). Source points
-// are accepted together before anything else: key (-inf, 0, -inf).
+// are accepted together before anything else: L = -inf (their t does not order them).
 #ifndef EIK_MAX_DEPTH
 #define EIK_MAX_DEPTH 4
 #endif
@@ -57,26 +57,67 @@ struct Key {
 EIK_HD bool key_le(const Key& a, const Key& b) {
   if (a.L != b.L) return a.L < b.L;
   if (a.d != b.d) return a.d < b.d;
+  if (a.L == -EIK_INF) return true;
   return a.t <= b.t;
 }
-EIK_HD bool key_eq(const Key& a, const Key& b) { return a.L == b.L && a.d == b.d && a.t == b.t; }
+EIK_HD bool key_eq(const Key& a, const Key& b) {
+  return a.L == b.L && a.d == b.d && (a.L == -EIK_INF || a.t == b.t);
+}
 EIK_HD Key key_normal(double t) { return Key{t, 0, t}; }
 EIK_HD Key key_source() { return Key{-EIK_INF, 0, -EIK_INF}; }
 EIK_HD Key key_unreached() { return Key{EIK_INF, 0, EIK_INF}; }
 EIK_HD bool key_reached(const Key& k) { return k.L < EIK_INF; }
 
-// Neighbourhood of one node as seen by the update. Index [axis][side]: side 0 is the
-// +1 neighbour (l=1 in the reference), side 1 the -1 neighbour (l=2).
+// Neighbourhood of one node as seen by the update, index [axis][side]: side 0 is the +1
+// neighbour (l=1 in the reference), side 1 the -1 neighbour (l=2). Compact so that the
+// whole record lives in registers: key levels as doubles, depths and flags as bit fields.
 struct Nbhd {
   double t1[3][2];   // traveltime at distance 1 (+inf if not reached / outside)
   double t2[3][2];   // traveltime at distance 2
-  Key k1[3][2];      // acceptance key at distance 1
-  Key k2[3][2];      // acceptance key at distance 2
-  bool in1[3][2];    // !isonb1: distance-1 node inside the grid
-  bool ok2[3][2];    // !isonb2 of the distance-1 node (2nd order allowed on that side)
+  double L1[3][2];   // key level at distance 1 (t for ordinary nodes, -inf for sources)
+  double L2[3][2];   // key level at distance 2
+  uint32_t d1, d2;   // key depths, 4 bits per slot (2*axis+side)
+  uint32_t in1;      // bit slot: distance-1 node inside the grid (!isonb1)
+  uint32_t ok2;      // bit slot: 2nd order allowed on that side (!isonb2 of the distance-1 node)
   double dh[3];      // node spacing per axis
   double slow;       // 1/vel at the node (computed as 1.0/vel, as the reference)
 };
+EIK_HD int slot(int a, int l) { return 2 * a + l; }
+EIK_HD Key nb_key1(const Nbhd& nb, int a, int l) {
+  return Key{nb.L1[a][l], (int)((nb.d1 >> (4 * slot(a, l))) & 15u), nb.t1[a][l]};
+}
+EIK_HD Key nb_key2(const Nbhd& nb, int a, int l) {
+  return Key{nb.L2[a][l], (int)((nb.d2 >> (4 * slot(a, l))) & 15u), nb.t2[a][l]};
+}
+EIK_HD bool nb_in1(const Nbhd& nb, int a, int l) { return (nb.in1 >> slot(a, l)) & 1u; }
+EIK_HD bool nb_ok2(const Nbhd& nb, int a, int l) { return (nb.ok2 >> slot(a, l)) & 1u; }
+EIK_HD void nb_clear(Nbhd& nb) {
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int l = 0; l < 2; l++) {
+      nb.t1[a][l] = EIK_INF;
+      nb.t2[a][l] = EIK_INF;
+      nb.L1[a][l] = EIK_INF;
+      nb.L2[a][l] = EIK_INF;
+    }
+  nb.d1 = nb.d2 = nb.in1 = nb.ok2 = 0u;
+}
+
+// Fill one slot: distance-1 node inside the grid (t, key level L, depth d).
+EIK_HD void nb_put1(Nbhd& nb, int a, int l, double t, double L, int d) {
+  nb.t1[a][l] = t;
+  nb.L1[a][l] = L;
+  nb.d1 |= (uint32_t)d << (4 * slot(a, l));
+  nb.in1 |= 1u << slot(a, l);
+}
+// Distance-2 node on a side where 2nd order is allowed.
+EIK_HD void nb_put2(Nbhd& nb, int a, int l, double t, double L, int d) {
+  nb.t2[a][l] = t;
+  nb.L2[a][l] = L;
+  nb.d2 |= (uint32_t)d << (4 * slot(a, l));
+  nb.ok2 |= 1u << slot(a, l);
+}
 
 // calcttpt_2ndord! with accepted(x) := key(x) <= T. codes receive the reference's
 // derivative codes (codeD): -side for 1st order, -2*side for 2nd order, 0 unused.
@@ -92,13 +133,13 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
 #pragma unroll
     for (int l = 0; l < 2; l++) {
       const int sh = l == 0 ? 1 : -1;
-      if (nb.in1[a][l] && key_le(nb.k1[a][l], T)) {
+      if (nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T)) {
         const double tv1 = nb.t1[a][l];
         if (tv1 < cv1) {
           cv1 = tv1;
           use1 = true;
           codes[a] = (int8_t)(-sh);
-          if (nb.ok2[a][l] && key_le(nb.k2[a][l], T)) {
+          if (nb_ok2(nb, a, l) && key_le(nb_key2(nb, a, l), T)) {
             const double tv2 = nb.t2[a][l];
             if (tv2 <= cv1) {
               cv2 = tv2;
@@ -140,7 +181,7 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
 #pragma unroll
       for (int l = 0; l < 2; l++) {
         const int sh = l == 0 ? 1 : -1;
-        if (nb.in1[a][l] && key_le(nb.k1[a][l], T)) {
+        if (nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T)) {
           const double tv1 = nb.t1[a][l];
           if (tv1 < cv1) {
             cv1 = tv1;
@@ -168,7 +209,7 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
 #pragma unroll
       for (int l = 0; l < 2; l++) {
         const int sh = l == 0 ? 1 : -1;
-        if (nb.in1[a][l] && key_le(nb.k1[a][l], T)) {
+        if (nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T)) {
           const double tv1 = nb.t1[a][l];
           if (tv1 < cv[a]) {
             cv[a] = tv1;
@@ -178,12 +219,20 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
       }
     }
     int id = 0;
+    double best = cv[0];
 #pragma unroll
     for (int a = 1; a < ND; a++)
-      if (cv[a] < cv[id]) id = a;
+      if (cv[a] < best) {
+        best = cv[a];
+        id = a;
+      }
+    double dhid = nb.dh[0];
+#pragma unroll
+    for (int a = 1; a < ND; a++)
+      if (a == id) dhid = nb.dh[a];
 #pragma unroll
     for (int a = 0; a < ND; a++) codes[a] = (a == id) ? cd[a] : (int8_t)0;
-    return (nb.dh[id] * nb.slow) + cv[id];
+    return (dhid * nb.slow) + best;
   }
   const double tmpsq = sqrt(sqarg);
   const double s1 = (-beta + tmpsq) / (2.0 * alpha);
@@ -191,43 +240,44 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
   return (s2 > s1) ? s2 : s1;
 }
 
-// Prefix rule: returns the node's traveltime (+inf if no neighbour is reached yet),
-// writes its derivative codes and its own acceptance key.
+// Smallest key of a reached in-grid immediate neighbour, strictly above lo if strict.
 template <int ND>
-EIK_HD double prefix_rule(const Nbhd& nb, int8_t* codes, Key* key_out, bool* negdisc) {
-  // distinct keys of the reached in-grid immediate neighbours, ascending
-  Key keys[2 * ND];
-  int nk = 0;
+EIK_HD void next_key_above(const Nbhd& nb, const Key& lo, bool strict, Key* out, bool* found) {
+  *found = false;
 #pragma unroll
   for (int a = 0; a < ND; a++)
 #pragma unroll
     for (int l = 0; l < 2; l++) {
-      const Key k = nb.k1[a][l];
-      if (nb.in1[a][l] && key_reached(k)) {
-        bool dup = false;
-        for (int q = 0; q < nk; q++)
-          if (key_eq(keys[q], k)) dup = true;
-        if (!dup) {
-          int p = nk;
-          while (p > 0 && !key_le(keys[p - 1], k)) {
-            keys[p] = keys[p - 1];
-            p--;
-          }
-          keys[p] = k;
-          nk++;
-        }
+      const Key k = nb_key1(nb, a, l);
+      if (!nb_in1(nb, a, l) || !key_reached(k)) continue;
+      if (strict && key_le(k, lo)) continue;
+      if (!*found || !key_le(*out, k)) {
+        *out = k;
+        *found = true;
       }
     }
+}
+
+// Prefix rule: returns the node's traveltime (+inf if no neighbour is reached yet),
+// writes its derivative codes and its own acceptance key. The groups of equal keys are
+// visited in increasing order by repeatedly taking the smallest neighbour key above the
+// previous one (no arrays: everything stays in registers on the GPU).
+template <int ND>
+EIK_HD double prefix_rule(const Nbhd& nb, int8_t* codes, Key* key_out, bool* negdisc) {
 #pragma unroll
   for (int a = 0; a < ND; a++) codes[a] = 0;
+  Key kg;
+  bool have;
+  next_key_above<ND>(nb, key_unreached(), false, &kg, &have);
   double vprev = EIK_INF;
   Key kprev = key_unreached();
   int8_t cprev[3] = {0, 0, 0};
-  for (int g = 0; g < nk; g++) {
+  bool first = true;
+#pragma unroll 1
+  for (int g = 0; g < 2 * ND && have; g++) {
     int8_t cg[3];
-    const double v = update_at<ND>(nb, keys[g], cg, negdisc);
-    const Key& kg = keys[g];
-    if (!(v > kg.L) && kg.d >= EIK_MAX_DEPTH && g > 0) {
+    const double v = update_at<ND>(nb, kg, cg, negdisc);
+    if (!(v > kg.L) && kg.d >= EIK_MAX_DEPTH && !first) {
       // A cascade of non-causal acceptances deeper than the heap ever produces: the
       // group is ordered after this node (transient of the iteration, not an FMM state).
 #pragma unroll
@@ -238,7 +288,10 @@ EIK_HD double prefix_rule(const Nbhd& nb, int8_t* codes, Key* key_out, bool* neg
     const Key mine = (v > kg.L) ? key_normal(v) : Key{kg.L, kg.d + 1, v};
 #pragma unroll
     for (int a = 0; a < ND; a++) codes[a] = cg[a];
-    if (g + 1 == nk || key_le(mine, keys[g + 1])) {
+    Key kn;
+    bool hn;
+    next_key_above<ND>(nb, kg, true, &kn, &hn);
+    if (!hn || key_le(mine, kn)) {
       *key_out = mine;
       return v;
     }
@@ -246,6 +299,8 @@ EIK_HD double prefix_rule(const Nbhd& nb, int8_t* codes, Key* key_out, bool* neg
     kprev = mine;
 #pragma unroll
     for (int a = 0; a < ND; a++) cprev[a] = cg[a];
+    kg = kn;
+    first = false;
   }
   *key_out = key_unreached();
   return EIK_INF;
