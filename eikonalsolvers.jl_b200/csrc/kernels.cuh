@@ -108,6 +108,7 @@ size_t fine_smem_bytes(int heapcap);
 void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs, int nprob,
                         const ForwardBatch& fb, const SolveArgs& sa, cudaStream_t st);
 void launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
+void launch_queue_init(const SolveArgs& sa, cudaStream_t st);  // empty queue, idle tiles, zero counters
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);
 

@@ -43,7 +43,7 @@ class eik_extra(C.Structure):
     _fields_ = [("refinearoundsrc", C.c_int32), ("downscalefactor", C.c_int32),
                 ("noderadius", C.c_int32), ("radiussmoothgradsrc", C.c_int32),
                 ("smoothgradkern", C.c_int32), ("parallelkind", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("nthreads", C.c_int32), ("reserved", C.c_int32)]
 
 
 class eik_stats(C.Structure):
@@ -110,9 +110,10 @@ def grid_struct(grd) -> eik_grid:
     return g
 
 
-def extra_struct(extraparams) -> eik_extra:
+def extra_struct(extraparams, nthreads: int = 1) -> eik_extra:
     e = eik_extra()
     load().eik_extra_defaults(C.byref(e))
+    e.nthreads = int(nthreads)
     if extraparams is not None:
         e.refinearoundsrc = int(extraparams.refinearoundsrc)
         e.downscalefactor = int(extraparams.grdrefpars.downscalefactor)

@@ -93,7 +93,14 @@ class Context:
             return out, [ttg[s * N:(s + 1) * N].reshape(grd.grsize, order="F").copy() for s in range(nsrc)]
         return out
 
-    def gradient(self, model: int, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad, extraparams=None):
+    def gradient(self, model: int, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad, extraparams=None,
+                 nthreads: int = 1):
+        """Misfit gradient for all sources in one batched device call.
+
+        ``nthreads`` stands for the caller's ``Threads.nthreads()``: under ``:sharedmem`` the
+        reference gives each of min(nsrc, nthreads) consecutive source groups its own gradient
+        buffer, which changes the values carried onto source points (eikmaingrad.jl:174-258).
+        """
         wg = whichgrad.lstrip(":") if isinstance(whichgrad, str) else whichgrad
         assert wg in WHICHGRAD, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)"
         cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
@@ -115,7 +122,7 @@ class Context:
         gv = np.zeros(N, dtype=np.float64) if wg in ("gradvel", "gradvelandsrcloc") else None
         gs = np.zeros(nsrc * grd.ndim, dtype=np.float64) if wg in ("gradsrcloc", "gradvelandsrcloc") else None
         misf = np.zeros(1, dtype=np.float64)
-        ep = _lib.extra_struct(extraparams)
+        ep = _lib.extra_struct(extraparams, nthreads)
         st = _lib.eik_stats()
         rc = self.L.eik_gradient(self.h, C.c_int64(model), nsrc, _lib.ptr(cs), _lib.ptr(recoff), _lib.ptr(rec),
                                  _lib.ptr(po), _lib.ptr(so), WHICHGRAD[wg], C.byref(ep), _lib.ptr(gv),
@@ -160,12 +167,13 @@ def eiktraveltime(vel, grd, coordsrc, coordrec, returntt: bool = False,
 
 
 def eikgradient(vel, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad,
-                extraparams: Optional[ExtraParams] = None, ctx: Optional[Context] = None):
+                extraparams: Optional[ExtraParams] = None, ctx: Optional[Context] = None,
+                nthreads: int = 1):
     """Gradient of the misfit w.r.t. velocity and/or source location, plus the misfit."""
     vel = np.asarray(vel, dtype=np.float64)
     assert 2 <= vel.ndim <= 3, "2<=ndims(vel)<=3"
     return _with_model(vel, grd, lambda c, m: c.gradient(m, grd, coordsrc, coordrec, pickobs, stdobs,
-                                                         whichgrad, extraparams), ctx)
+                                                         whichgrad, extraparams, nthreads), ctx)
 
 
 def eikttimemisfit(velmod, grd, coordsrc, coordrec, ttpicksobs, stdobs,

@@ -83,7 +83,11 @@ typedef struct {
   int32_t radiussmoothgradsrc;  /* default 3 */
   int32_t smoothgradkern;       /* default 0 (odd when > 0) */
   int32_t parallelkind;         /* 0 serial, 1 sharedmem, 2 distribmem */
-  int32_t reserved[2];
+  int32_t nthreads;             /* Threads.nthreads() of the caller; with :sharedmem the
+                                   gradient's sources form min(nsrc, nthreads) consecutive
+                                   groups with separate gradient buffers (distribsrcs,
+                                   eikutils.jl:171-190). 0 or 1: one group. */
+  int32_t reserved;
 } eik_extra;
 
 typedef struct {
