@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark of the forward + discrete-adjoint path: gradient source-solves/s.
+
+Workload (default): 3D Cartesian eikgradient :gradvelandsrcloc on 256^3 nodes, hgrid 0.1,
+4-layer velocity (3.0/4.2/5.5/6.8) with seeded sinusoidal interfaces plus 2% white
+perturbation, 32 sources in the lower half, 400 receivers on a 20x20 surface grid,
+observations from a 5%-perturbed model plus N(0, 0.01^2) noise, default ExtraParams
+(refined start-up ds=5 r=3, source smoothing radius 3). All inputs are seeded synthetic.
+
+One step = one batched gradient call over the rank's sources (forward FMM fixed point,
+adjoint dataflow solve, gradient assembly). Every per-source field is 134 MB and the
+working set is tens of GB, far above the 126 MB L2, so no flush is needed between steps.
+
+Lines printed by rank 0 (one JSON object):
+  value     source-solves/s of the whole job, inputs resident on the device (C-ABI
+            eik_gradient_device), timed with CUDA events on the library's stream
+  e2e       the same through eik_gradient with pinned host buffers, host<->device copies
+            inside the timed region
+  plain     the same workload one source per call (the unbatched path)
+  roofline  HBM roofline of the dominant kernel (algorithmic bytes / measured duration)
+  cpu_baseline  the oracle (C++ restatement of the reference algorithm) on the host cores
+
+--impl reference: times the oracle on the host cores instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "eikonalsolvers.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "gradient source-solves/s @256^3 batched vs plain GPU; p50/p99 serve latency"
+UNIT = "source-solves/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="grid scale (1.0 = 256^3)")
+    ap.add_argument("--nsrc", type=int, default=32, help="sources per rank")
+    ap.add_argument("--plain-sources", type=int, default=2,
+                    help="sources timed one per call for the plain path (0 = skip)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------ helpers --
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch of a kernel from a committed ncu summary, if one exists:
+    a line `traffic_bytes_per_source_solve: <float>` in profiles/<name>.md."""
+    p = os.path.join(REPO, "profiles", name + ".md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_bytes_per_source_solve:\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 9 and parts[1].replace(".", "").isdigit():
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def host_cores(cap=32):
+    """Host threads for the CPU leg: all cores this process may use, at most `cap` and at
+    most one per 1.5 GB of available RAM (the oracle holds ~1 GB per 128^3 gradient)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+        n = min(n, max(1, int(avail / 1.5e9)))
+    except (ValueError, OSError):
+        pass
+    return max(1, min(n, cap))
+
+
+# ------------------------------------------------------------------- workloads --
+def make_workload(scale, nsrc_total, forward=None):
+    from eikonalsolvers import configs as CF
+    return CF.cfg3(scale=scale, nsrc=nsrc_total, forward=forward, nrec_side=20)
+
+
+def flat_inputs(w, s0, s1):
+    cs = np.ascontiguousarray(w.coordsrc[s0:s1], dtype=np.float64)
+    recs = w.coordrec[s0:s1]
+    off = np.zeros(len(recs) + 1, dtype=np.int64)
+    for i, r in enumerate(recs):
+        off[i + 1] = off[i] + r.shape[0]
+    rec = np.ascontiguousarray(np.concatenate(recs), dtype=np.float64)
+    po = np.ascontiguousarray(np.concatenate(w.pickobs[s0:s1]), dtype=np.float64)
+    so = np.ascontiguousarray(np.concatenate(w.stdobs[s0:s1]), dtype=np.float64)
+    return cs, off, rec, po, so
+
+
+# ----------------------------------------------------------------- CPU leg (oracle) --
+def cpu_sample(w, nthreads, nsrc):
+    """Bounded CPU sample of the workload for the oracle: a 128^3 sub-block of the model
+    (x, y nodes 64..191, z nodes 128..255: the lower half where the sources are) with the
+    workload's sources mapped into it and a 20x20 receiver grid on its top face."""
+    from eikonalsolvers import Grid3DCart
+    n = w.grd.grsize[0]
+    b = n // 2
+    lo = np.array([n // 4, n // 4, n // 2])
+    vel = np.ascontiguousarray(w.vel[lo[0]:lo[0] + b, lo[1]:lo[1] + b, lo[2]:lo[2] + b])
+    h = w.grd.hgrid
+    grd = Grid3DCart(hgrid=h, cooinit=(0.0, 0.0, 0.0), grsize=(b, b, b))
+    ext = (b - 1) * h
+    src = []
+    for s in range(nsrc):
+        x, y, z = w.coordsrc[s % len(w.coordsrc)]
+        full = (n - 1) * h
+        src.append([0.05 * ext + 0.9 * ext * x / full, 0.05 * ext + 0.9 * ext * y / full,
+                    min(max(z - lo[2] * h, 0.05 * ext), 0.95 * ext)])
+    xr = np.linspace(0.0, ext, 20)
+    rec = np.array([[a, c, 0.0] for c in xr for a in xr])
+    return vel, grd, np.array(src), [rec.copy() for _ in range(nsrc)], (b / n) ** 3
+
+
+def run_cpu_leg(w, steps, warmup, nthreads):
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import eikoracle as O
+    from eikonalsolvers import ExtraParams
+    nsrc = nthreads
+    vel, grd, cs, rec, frac = cpu_sample(w, nthreads, nsrc)
+    ep = ExtraParams(parallelkind="sharedmem")
+    picks = O.eiktraveltime(vel * 1.02, grd, cs, rec, extraparams=ep, nthreads=nthreads)
+    std = [0.01 * np.ones(p.shape) for p in picks]
+    times = []
+    for it in range(warmup + steps):
+        t0 = time.perf_counter()
+        O.eikgradient(vel, grd, cs, rec, picks, std, "gradvelandsrcloc", extraparams=ep, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        if it >= warmup:
+            times.append(dt)
+    t = sum(times) / len(times)
+    value = nsrc / t * frac
+    sample = (f"{nsrc} sources (one per thread) of the workload on a {grd.grsize[0]}^3 sub-block of its "
+              f"model, gradvelandsrcloc, {t:.2f} s per call; source-solves/s scaled to 256^3 by node count "
+              f"(x{frac:.4g})")
+    return value, sample
+
+
+# ----------------------------------------------------------------------- GPU arm --
+def main_b200(args):
+    import torch
+    import torch.distributed as dist
+    from eikonalsolvers import Context, ExtraParams
+    from eikonalsolvers import _lib
+
+    ws, rank, local = dist_env()
+    if args.gpus > 1 and ws == 1:
+        print(json.dumps({"error": "run --gpus N>1 under torch.distributed.run"}))
+        return 2
+    torch.cuda.set_device(local)
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    ctx = Context(local)
+    L = ctx.L
+
+    # ---- workload: every rank takes its own contiguous block of sources
+    nsrc = args.nsrc
+    w = make_workload(args.scale, nsrc * ws)
+    s0, s1 = rank * nsrc, (rank + 1) * nsrc
+    ep = ExtraParams()
+    mid_obs = ctx.upload(w.vel_obs, w.grd)
+    picks = ctx.traveltime(mid_obs, w.grd, w.coordsrc[s0:s1], w.coordrec[s0:s1], extraparams=ep)
+    ctx.release(mid_obs)
+    rng = np.random.default_rng(12 + rank)
+    w.pickobs = [None] * (nsrc * ws)
+    w.stdobs = [None] * (nsrc * ws)
+    for i, p in enumerate(picks):
+        w.pickobs[s0 + i] = p + rng.normal(0.0, 0.01, p.shape)
+        w.stdobs[s0 + i] = 0.01 * np.ones(p.shape)
+    mid = ctx.upload(w.vel, w.grd)
+    N = int(np.prod(w.grd.grsize))
+    nd = w.grd.ndim
+    cs, off, rec, po, so = flat_inputs(w, s0, s1)
+    d_cs = torch.from_numpy(cs).to(dev)
+    d_rec = torch.from_numpy(rec).to(dev)
+    d_po = torch.from_numpy(po).to(dev)
+    d_so = torch.from_numpy(so).to(dev)
+    d_gv = torch.empty(N, dtype=torch.float64, device=dev)
+    d_gs = torch.empty(nsrc * nd, dtype=torch.float64, device=dev)
+    d_m = torch.empty(1, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+    epc = _lib.extra_struct(ep)
+    stream = torch.cuda.ExternalStream(L.eik_ctx_stream(ctx.h), device=dev)
+    P = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def step(st):
+        rc = L.eik_gradient_device(ctx.h, C.c_int64(mid), nsrc, P(d_cs), _lib.ptr(off), P(d_rec), P(d_po),
+                                   P(d_so), 3, C.byref(epc), P(d_gv), P(d_gs), P(d_m), C.byref(st))
+        _lib.check(rc, ctx.h)
+        if ws > 1:  # the gradient of the whole job is the sum over the ranks' sources
+            with torch.cuda.stream(stream):
+                dist.all_reduce(d_gv)
+                dist.all_reduce(d_m)
+
+    st = _lib.eik_stats()
+    for _ in range(args.warmup):
+        step(st)
+    # ---- timed region (device-resident inputs)
+    fine_ms = solve_ms = adj_ms = 0.0
+    launches = 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(st)
+            fine_ms += st.fine_ms
+            solve_ms += st.solve_ms
+            adj_ms += st.adj_ms
+            launches += st.launches
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = nsrc * ws * args.steps / (ms_max / 1000.0)
+    clocks = clk.summary()
+
+    # ---- end to end through the host C-ABI entry point, pinned host buffers
+    h_cs, h_off, h_rec, h_po, h_so = (torch.from_numpy(a).pin_memory() for a in (cs, off, rec, po, so))
+    h_gv = torch.empty(N, dtype=torch.float64).pin_memory()
+    h_gs = torch.empty(nsrc * nd, dtype=torch.float64).pin_memory()
+    h_m = C.c_double()
+    st2 = _lib.eik_stats()
+    Ph = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.e2e_steps):
+        rc = L.eik_gradient(ctx.h, C.c_int64(mid), nsrc, Ph(h_cs), Ph(h_off), Ph(h_rec), Ph(h_po), Ph(h_so), 3,
+                            C.byref(epc), Ph(h_gv), Ph(h_gs), C.byref(h_m), C.byref(st2))
+        _lib.check(rc, ctx.h)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = nsrc * ws * args.e2e_steps / (float(t.item()) / 1000.0)
+    h2d = cs.nbytes + off.nbytes + rec.nbytes + po.nbytes + so.nbytes
+    d2h = N * 8 + nsrc * nd * 8 + 8
+
+    # ---- plain path: one source per call
+    plain = None
+    if args.plain_sources > 0:
+        npl = min(args.plain_sources, nsrc)
+        stp = _lib.eik_stats()
+        offs = [np.array([0, off[i + 1] - off[i]], dtype=np.int64) for i in range(npl)]
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for i in range(npl):
+            r0 = int(off[i])
+            rc = L.eik_gradient_device(ctx.h, C.c_int64(mid), 1, C.c_void_p(d_cs.data_ptr() + 8 * nd * i),
+                                       _lib.ptr(offs[i]), C.c_void_p(d_rec.data_ptr() + 8 * nd * r0),
+                                       C.c_void_p(d_po.data_ptr() + 8 * r0), C.c_void_p(d_so.data_ptr() + 8 * r0),
+                                       3, C.byref(epc), P(d_gv), C.c_void_p(d_gs.data_ptr() + 8 * nd * i), P(d_m),
+                                       C.byref(stp))
+            _lib.check(rc, ctx.h)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([g0.elapsed_time(g1)], dtype=torch.float64, device=dev)
+        if ws > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        pv = npl * ws / (float(t.item()) / 1000.0)
+        plain = {"value": pv, "unit": UNIT, "sources_timed_per_rank": npl, "batched_over_plain": value / pv}
+
+    # ---- roofline of the dominant kernel (measured inside the timed region)
+    peak, peak_kind = measured_peaks()
+    kern = {"coarse_solve_kernel": (solve_ms, 16), "adj_solve_kernel": (adj_ms, 16),
+            "fine_fmm_kernel": (fine_ms, 16)}
+    top = max(kern, key=lambda k: kern[k][0])
+    kms, bpn = kern[top]
+    per_launch_ms = kms / args.steps
+    alg_bytes = bpn * N * nsrc  # per launch: one launch serves all the rank's sources
+    achieved = alg_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic_ss = profile_traffic(top)
+    roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind,
+            "traffic": (traffic_ss * nsrc if traffic_ss is not None else None),
+            "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms,
+            "share_of_step": kms / ms,
+            "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()}}
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        cores = host_cores()
+        v, sample = run_cpu_leg(w, steps=1, warmup=0, nthreads=cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": f"3D Cartesian eikgradient :gradvelandsrcloc, {w.grd.grsize[0]}^3, "
+                                   f"hgrid {w.grd.hgrid}, 4-layer model, {nsrc} sources per GPU, 400 receivers, "
+                                   "default ExtraParams (refined start-up ds=5 r=3, smoothing radius 3)",
+                       "sources_per_gpu": nsrc, "nodes": N, "parallelism": f"sources sharded over {ws} GPU(s)",
+                       "l2": "inputs and per-source fields far larger than L2 (no flush)"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "steps": args.e2e_steps},
+            "plain": plain,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+            "stats": {"tile_activations": int(st.tile_activations), "node_evals": int(st.node_evals),
+                      "adj_activations": int(st.adj_activations), "evals_per_node": st.node_evals / (N * nsrc)},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.release(mid)
+    ctx.close()
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    cores = host_cores()
+    w = make_workload(args.scale, args.nsrc)
+    v, sample = run_cpu_leg(w, steps=args.steps, warmup=args.warmup, nthreads=cores)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "oracle (C++ restatement of the reference FMM + CSR adjoint), "
+                                   "threaded by source groups as :sharedmem"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    a = parse()
+    sys.exit(main_reference(a) if a.impl == "reference" else main_b200(a))

@@ -1015,71 +1015,69 @@ static void launch_adj_solve(const AdjArgs& aa, int nsm, cudaStream_t st) {
 
 using namespace eik;
 
-#define CUDA_OK2(ctx, call)                                                            \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess) return fail(ctx, EIK_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
-  } while (0)
 
-extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
-                            const int64_t* rec_off, const double* rec, const double* pickobs,
-                            const double* stdobs, int32_t whichgrad, const eik_extra* ep_in, double* gradvel,
-                            double* gradsrc, double* misfit, eik_stats* stats) {
-  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  auto it = ctx->models.find(model);
-  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
-  const Model& m = it->second;
-  eik_extra ep;
-  if (ep_in) ep = *ep_in;
-  else eik_extra_defaults(&ep);
+
+// Per-source misfits summed as the reference does: 0.5*m per source within a group, then
+// over the groups (eikmaingrad.jl:137-150, 241).
+__global__ void adj_misfit_kernel(const double* misf, int nsrc, int nw, double* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double tot = 0.0, acc = 0.0;
+  int gcur = 0;
+  bool first_group = true;
+  for (int s = 0; s < nsrc; s++) {
+    const int gs = group_start(nsrc, nw, s);
+    if (s > 0 && gs != gcur) {
+      tot = first_group ? acc : tot + acc;
+      first_group = false;
+      acc = 0.0;
+      gcur = gs;
+    }
+    acc += 0.5 * misf[s];
+  }
+  *out = first_group ? acc : tot + acc;
+}
+
+namespace eik {
+
+static int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichgrad, const eik_extra& ep) {
   if (whichgrad < 1 || whichgrad > 3)
     return fail(ctx, EIK_ERR_ASSERT, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)");
   int rc = check_extra(ctx, &ep);
   if (rc) return rc;
   if (ep.smoothgradkern > 0)
     return fail(ctx, EIK_ERR_UNSUPPORTED, "smoothgradkern>0 (Gaussian smoothing of the summed gradient) is not built");
-  if (stats) std::memset(stats, 0, sizeof *stats);
   if (nsrc <= 0) return fail(ctx, EIK_ERR_ASSERT, "nsrc >= 1");
-  if (!coordsrc || !rec_off || !rec || !pickobs || !stdobs) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
   if ((whichgrad == 2 || whichgrad == 3) && !is_cart(m.g))
     return fail(ctx, EIK_ERR_ERROR, "type %s has no field hgrid", m.g.nd == 2 ? "Grid2DSphere" : "Grid3DSphere");
-  rc = check_positions(ctx, m.g, nsrc, coordsrc, rec_off, rec);
-  if (rc) return rc;
   for (int a = 0; a < m.g.nd; a++)
     if (m.g.n[a] < 3) return fail(ctx, EIK_ERR_ERROR, "BoundsError: grid axis %d has fewer than 3 nodes", a);
-  CUDA_OK2(ctx, cudaSetDevice(ctx->device));
+  return EIK_OK;
+}
+
+// Forward + adjoint + assembly for nsrc sources whose inputs are on the device.
+// Outputs (each nullable): d_gradvel N values, d_gradsrc nsrc x nd, d_misfit 1 value.
+// Returns after the stream has drained and the device error word has been checked.
+static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
+                         const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
+                         const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit,
+                         eik_stats* stats) {
+  int rc = EIK_OK;
   cudaStream_t st = ctx->stream;
   Scratch& S = ctx->scratch;
   const int nd = m.g.nd;
-  const long long N = m.N, nrec = rec_off[nsrc];
+  const long long N = m.N;
   // :sharedmem splits the sources into groups with separate gradient buffers
   const int ngroups = (ep.parallelkind == 1 && ep.nthreads > 1) ? ep.nthreads : 1;
+  const bool wantvel = whichgrad == 1 || whichgrad == 3;
+  ForwardState fw;
+  rc = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
+  if (rc) return rc;
 #define GET(var, type, name, count)                                                  \
   var = (type*)S.get(name, sizeof(type) * (size_t)(count), &rc);                     \
   if (!var) return rc == EIK_ERR_OUT_OF_BUDGET                                       \
                      ? fail(ctx, rc, "scratch '%s' exceeds the HBM budget", name)    \
                      : fail(ctx, rc, "cudaMalloc of scratch '%s' failed", name);
-  double *d_cs, *d_rec, *d_po, *d_so;
-  long long* d_off;
-  GET(d_cs, double, "in_cs", nsrc * nd);
-  GET(d_off, long long, "in_off", nsrc + 1);
-  GET(d_rec, double, "in_rec", std::max<long long>(nrec, 1) * nd);
-  GET(d_po, double, "in_pickobs", std::max<long long>(nrec, 1));
-  GET(d_so, double, "in_stdobs", std::max<long long>(nrec, 1));
-  cudaEventRecord(ctx->ev0, st);
-  CUDA_OK2(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
-  CUDA_OK2(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
-  if (nrec) {
-    CUDA_OK2(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
-    CUDA_OK2(ctx, cudaMemcpyAsync(d_po, pickobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
-    CUDA_OK2(ctx, cudaMemcpyAsync(d_so, stdobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
-  }
-  ForwardState fw;
-  rc = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
-  if (rc) return rc;
-  // adjoint state
-  double *lam, *gdt, *rhs, *misf, *dpsi, *ysrc, *gnode, *gsrc, *flam, *carry, *gtot;
+  double *lam, *gdt, *rhs, *misf, *dpsi, *ysrc, *gnode, *gsrc, *flam, *fgdt, *carry;
   AdjProblem* dap;
   ForwardBatch* dfb;
   uint32_t* dwarn;
@@ -1093,9 +1091,7 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
   GET(carry, double, "adj_carry", nsrc * fw.fb.seedcap);
   GET(gsrc, double, "adj_gsrc", nsrc * nd);
   GET(flam, double, "adj_fine_lam", ep.refinearoundsrc ? nsrc * fw.fb.nfmax : 1);
-  double* fgdt;
   GET(fgdt, double, "adj_fine_gdt", ep.refinearoundsrc ? nsrc * nd * fw.fb.nfmax : 1);
-  GET(gtot, double, "adj_gtot", N);
   GET(dap, AdjProblem, "adj_probs", nsrc);
   GET(dfb, ForwardBatch, "adj_fb", 1);
   GET(dwarn, uint32_t, "adj_warn", 1);
@@ -1106,10 +1102,10 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
     hap[s].gdt = gdt + s * N * nd;
     hap[s].rhs = rhs + s * N;
   }
-  CUDA_OK2(ctx, cudaMemcpyAsync(dap, hap.data(), sizeof(AdjProblem) * nsrc, cudaMemcpyHostToDevice, st));
-  CUDA_OK2(ctx, cudaMemcpyAsync(dfb, &fw.fb, sizeof(ForwardBatch), cudaMemcpyHostToDevice, st));
-  CUDA_OK2(ctx, cudaMemsetAsync(dwarn, 0, sizeof(uint32_t), st));
-  CUDA_OK2(ctx, cudaMemsetAsync(gsrc, 0, sizeof(double) * nsrc * nd, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(dap, hap.data(), sizeof(AdjProblem) * nsrc, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(dfb, &fw.fb, sizeof(ForwardBatch), cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemsetAsync(dwarn, 0, sizeof(uint32_t), st));
+  CUDA_OK(ctx, cudaMemsetAsync(gsrc, 0, sizeof(double) * nsrc * nd, st));
   const CoarseProblem* dprobs = fw.sa.probs;
   adj_prep_kernel<<<2 * ctx->nsm * 8, 256, 0, st>>>(dprobs, dap, (int)nsrc, N);
   RecvArgs ra;
@@ -1134,15 +1130,18 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
   aa.sa.node_evals = fw.sa.activations + 5;
   launch_queue_init(aa.sa, st);
   adj_seed_kernel<<<ctx->nsm * 4, 256, 0, st>>>(aa.sa, (int)nsrc);
+  cudaEventRecord(ctx->evk[4], st);
   if (nd == 3) launch_adj_solve<3>(aa, ctx->nsm, st);
   else launch_adj_solve<2>(aa, ctx->nsm, st);
+  cudaEventRecord(ctx->evk[5], st);
   adj_check_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, N, fw.fb.err);
-  CUDA_OK2(ctx, cudaGetLastError());
+  CUDA_OK(ctx, cudaGetLastError());
   SrcTermArgs ta;
   ta.g = m.g;
   ta.nsrc = (int)nsrc;
   ta.refine = ep.refinearoundsrc;
   ta.whichgrad = whichgrad;
+  ta.ngroups = ngroups;
   ta.probs = dprobs;
   ta.ap = dap;
   ta.fb = dfb;
@@ -1154,47 +1153,149 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
   ta.gradsrc = gsrc;
   ta.fine_lam = flam;
   ta.fine_gdt = fgdt;
-  ta.ngroups = ngroups;
   ta.warn = dwarn;
   adj_ysrc_kernel<<<(int)nsrc, 128, 0, st>>>(ta);
   adj_srcterm_kernel<<<(int)nsrc, 32, 0, st>>>(ta);
-  if (whichgrad == 1 || whichgrad == 3) {
+  if (wantvel) {
     adj_field_kernel<<<ctx->nsm * 8, 256, 0, st>>>(ta, N);
     adj_carry_kernel<<<(int)nsrc, 64, 0, st>>>(ta, ep.radiussmoothgradsrc, carry);
     adj_srcnodes_kernel<<<(int)nsrc, 128, 0, st>>>(ta, carry);
     if (ep.radiussmoothgradsrc > 0) adj_smooth_kernel<<<(int)nsrc, 256, 0, st>>>(ta, ep.radiussmoothgradsrc);
-    adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ngroups, N, gtot);
+    if (d_gradvel) adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ngroups, N, d_gradvel);
   }
-  CUDA_OK2(ctx, cudaGetLastError());
-  std::vector<double> hm(nsrc);
-  CUDA_OK2(ctx, cudaMemcpyAsync(hm.data(), misf, sizeof(double) * nsrc, cudaMemcpyDeviceToHost, st));
-  if (gradvel && (whichgrad == 1 || whichgrad == 3))
-    CUDA_OK2(ctx, cudaMemcpyAsync(gradvel, gtot, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
-  if (gradsrc && (whichgrad == 2 || whichgrad == 3))
-    CUDA_OK2(ctx, cudaMemcpyAsync(gradsrc, gsrc, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToHost, st));
+  if (d_misfit) adj_misfit_kernel<<<1, 1, 0, st>>>(misf, (int)nsrc, ngroups, d_misfit);
+  if (d_gradsrc && whichgrad != 1)
+    CUDA_OK(ctx, cudaMemcpyAsync(d_gradsrc, gsrc, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToDevice, st));
+  CUDA_OK(ctx, cudaGetLastError());
   uint32_t hw = 0;
-  CUDA_OK2(ctx, cudaMemcpyAsync(&hw, dwarn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  cudaEventRecord(ctx->ev1, st);
+  unsigned long long actr[2] = {0, 0};
+  CUDA_OK(ctx, cudaMemcpyAsync(&hw, dwarn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(actr, aa.sa.activations, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   rc = collect_forward_stats(ctx, &fw, stats);
   if (stats) {
     stats->warn_mask |= hw;
+    stats->adj_activations = actr[0];
+    stats->launches += 8 + (d_misfit ? 1 : 0) +
+                       (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->evk[4], ctx->evk[5]);
+    stats->adj_ms = ms;
+  }
+  return rc;
+}
+
+}  // namespace eik
+
+extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
+                            const int64_t* rec_off, const double* rec, const double* pickobs,
+                            const double* stdobs, int32_t whichgrad, const eik_extra* ep_in, double* gradvel,
+                            double* gradsrc, double* misfit, eik_stats* stats) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->models.find(model);
+  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  const Model& m = it->second;
+  eik_extra ep;
+  if (ep_in) ep = *ep_in;
+  else eik_extra_defaults(&ep);
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  int rc = validate_gradient(ctx, m, nsrc, whichgrad, ep);
+  if (rc) return rc;
+  if (!coordsrc || !rec_off || !rec || !pickobs || !stdobs) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  rc = check_positions(ctx, m.g, nsrc, coordsrc, rec_off, rec);
+  if (rc) return rc;
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  Scratch& S = ctx->scratch;
+  const int nd = m.g.nd;
+  const long long N = m.N, nrec = rec_off[nsrc];
+#define GET(var, type, name, count)                                                  \
+  var = (type*)S.get(name, sizeof(type) * (size_t)(count), &rc);                     \
+  if (!var) return rc == EIK_ERR_OUT_OF_BUDGET                                       \
+                     ? fail(ctx, rc, "scratch '%s' exceeds the HBM budget", name)    \
+                     : fail(ctx, rc, "cudaMalloc of scratch '%s' failed", name);
+  double *d_cs, *d_rec, *d_po, *d_so, *d_gv, *d_gs, *d_m;
+  long long* d_off;
+  GET(d_cs, double, "in_cs", nsrc * nd);
+  GET(d_off, long long, "in_off", nsrc + 1);
+  GET(d_rec, double, "in_rec", std::max<long long>(nrec, 1) * nd);
+  GET(d_po, double, "in_pickobs", std::max<long long>(nrec, 1));
+  GET(d_so, double, "in_stdobs", std::max<long long>(nrec, 1));
+  GET(d_gv, double, "out_gradvel", N);
+  GET(d_gs, double, "out_gradsrc", nsrc * nd);
+  GET(d_m, double, "out_misfit", 1);
+#undef GET
+  cudaEventRecord(ctx->ev0, st);
+  CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
+  if (nrec) {
+    CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
+    CUDA_OK(ctx, cudaMemcpyAsync(d_po, pickobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
+    CUDA_OK(ctx, cudaMemcpyAsync(d_so, stdobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
+  }
+  const bool wantvel = whichgrad == 1 || whichgrad == 3, wantsrc = whichgrad != 1;
+  rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
+                     wantsrc ? d_gs : nullptr, d_m, stats);
+  if (rc) return rc;
+  double hm = 0.0;
+  CUDA_OK(ctx, cudaMemcpyAsync(&hm, d_m, sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (gradvel && wantvel) CUDA_OK(ctx, cudaMemcpyAsync(gradvel, d_gv, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  if (gradsrc && wantsrc)
+    CUDA_OK(ctx, cudaMemcpyAsync(gradsrc, d_gs, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToHost, st));
+  cudaEventRecord(ctx->ev1, st);
+  CUDA_OK(ctx, cudaStreamSynchronize(st));
+  if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     stats->device_ms = ms;
   }
+  if (misfit) *misfit = hm;
+  return EIK_OK;
+}
+
+extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc_dev,
+                                   const int64_t* rec_off, const double* rec_dev, const double* pickobs_dev,
+                                   const double* stdobs_dev, int32_t whichgrad, const eik_extra* ep_in,
+                                   double* gradvel_dev, double* gradsrc_dev, double* misfit_dev,
+                                   eik_stats* stats) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->models.find(model);
+  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  const Model& m = it->second;
+  eik_extra ep;
+  if (ep_in) ep = *ep_in;
+  else eik_extra_defaults(&ep);
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  int rc = validate_gradient(ctx, m, nsrc, whichgrad, ep);
   if (rc) return rc;
-  if (misfit) {  // per group in source order, then over groups (eikmaingrad.jl:137-150)
-    const int64_t nw = ngroups;
-    const int64_t ng = (nw <= 1) ? 1 : std::min<int64_t>(nsrc, nw);
-    double tot = 0.0;
-    int64_t s = 0;
-    for (int64_t gi = 0; gi < ng; gi++) {
-      const int64_t sz = (ng == 1) ? nsrc : (nsrc < nw ? 1 : nsrc / nw + (gi < nsrc % nw ? 1 : 0));
-      double acc = 0.0;
-      for (int64_t q = 0; q < sz; q++, s++) acc += 0.5 * hm[s];
-      tot = (gi == 0) ? acc : tot + acc;
-    }
-    *misfit = tot;
+  if (!coordsrc_dev || !rec_off || !rec_dev || !pickobs_dev || !stdobs_dev)
+    return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int nd = m.g.nd;
+  const long long nrec = rec_off[nsrc];
+  // positions are checked on the host, as the reference does before any solve
+  std::vector<double> hcs((size_t)nsrc * nd), hrec((size_t)std::max<long long>(nrec, 1) * nd);
+  cudaEventRecord(ctx->ev0, st);
+  CUDA_OK(ctx, cudaMemcpyAsync(hcs.data(), coordsrc_dev, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToHost, st));
+  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(hrec.data(), rec_dev, sizeof(double) * nrec * nd, cudaMemcpyDeviceToHost, st));
+  CUDA_OK(ctx, cudaStreamSynchronize(st));
+  rc = check_positions(ctx, m.g, nsrc, hcs.data(), rec_off, hrec.data());
+  if (rc) return rc;
+  long long* d_off = (long long*)ctx->scratch.get("in_off", sizeof(long long) * (nsrc + 1), &rc);
+  if (!d_off) return fail(ctx, rc, "scratch allocation failed");
+  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
+  rc = gradient_core(ctx, m, nsrc, coordsrc_dev, d_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad, ep,
+                     (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
+                     misfit_dev, stats);
+  if (rc) return rc;
+  cudaEventRecord(ctx->ev1, st);
+  CUDA_OK(ctx, cudaStreamSynchronize(st));
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->device_ms = ms;
   }
   return EIK_OK;
 }

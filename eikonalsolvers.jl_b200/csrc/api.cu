@@ -31,12 +31,7 @@ int fail(eik_ctx* ctx, int code, const char* fmt, ...) {
   return code;
 }
 
-#define CUDA_OK(ctx, call)                                                                      \
-  do {                                                                                          \
-    cudaError_t e_ = (call);                                                                    \
-    if (e_ != cudaSuccess)                                                                      \
-      return fail(ctx, EIK_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));           \
-  } while (0)
+
 
 // -------------------------------------------------------------------- scratch --
 void* Scratch::get(const std::string& name, size_t bytes, int* rc) {
@@ -330,12 +325,16 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   CUDA_OK(ctx, cudaMemcpyAsync(dp, hp.data(), sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.err, 0, sizeof(uint32_t) * 4, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.out, 0, sizeof(SrcOut) * nsrc, st));
+  cudaEventRecord(ctx->evk[0], st);
   if (refine) launch_fine(fb, st);
   else launch_srcbox(fb, st);
+  cudaEventRecord(ctx->evk[1], st);
   CUDA_OK(ctx, cudaGetLastError());
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
   CUDA_OK(ctx, cudaGetLastError());
+  cudaEventRecord(ctx->evk[2], st);
   launch_coarse_solve(sa, ctx->nsm, st);
+  cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
   fw->fb = fb;
   fw->sa = sa;
@@ -345,7 +344,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   fw->kd = kd;
   fw->N = N;
   fw->nsrc = nsrc;
-  (void)stats;
+  if (stats) stats->launches += 5;  // start-up, init, queue init, seeds, solve
   return EIK_OK;
 }
 
@@ -364,6 +363,11 @@ int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
     stats->err_mask |= e;
     stats->tile_activations += ctr[2];
     stats->node_evals += ctr[3];
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ctx->evk[0], ctx->evk[1]);
+    cudaEventElapsedTime(&b, ctx->evk[2], ctx->evk[3]);
+    stats->fine_ms = a;
+    stats->solve_ms = b;
   }
   fw->host_out = std::move(outs);
   return err_to_rc(ctx, e);
@@ -406,6 +410,7 @@ int eik_ctx_create(int device, size_t hbm_budget, eik_ctx** out) {
   }
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);
+  for (auto& e : c->evk) cudaEventCreate(&e);
   *out = c;
   return EIK_OK;
 }
@@ -421,10 +426,13 @@ int eik_ctx_destroy(eik_ctx* ctx) {
   ctx->scratch.release_all();
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
+  for (auto& e : ctx->evk) cudaEventDestroy(e);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return EIK_OK;
 }
+
+void* eik_ctx_stream(eik_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 const char* eik_last_error(eik_ctx* ctx) {
   (void)ctx;
@@ -494,6 +502,7 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
   rc = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
   if (rc) return rc;
   if (nrec) launch_picks(m.g, fw.t, m.N, (int)nsrc, d_off, d_rec, d_picks, st);
+  if (nrec && stats) stats->launches += 1;
   CUDA_OK(ctx, cudaGetLastError());
   if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
   if (ttgrids)

@@ -11,6 +11,13 @@
 #include "../../include/eikcuda.h"
 #include "kernels.cuh"
 
+#define CUDA_OK(ctx, call)                                                                      \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return eik::fail(ctx, EIK_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_));      \
+  } while (0)
+
 namespace eik {
 
 // Grow-only named device buffers, bounded by the context's HBM budget.
@@ -62,7 +69,8 @@ struct eik_ctx {
   int device = 0;
   int nsm = 148;
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // whole call
+  cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
   std::mutex mu;
   eik::Scratch scratch;
   size_t model_bytes = 0;

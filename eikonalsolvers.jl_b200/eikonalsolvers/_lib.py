@@ -21,7 +21,7 @@ ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EI
 
 EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last_error",
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
-            "eik_gradient"]
+            "eik_gradient", "eik_gradient_device", "eik_ctx_stream"]
 
 
 class EikError(RuntimeError):
@@ -48,7 +48,9 @@ class eik_extra(C.Structure):
 
 class eik_stats(C.Structure):
     _fields_ = [("warn_mask", C.c_uint32), ("err_mask", C.c_uint32), ("tile_activations", C.c_uint64),
-                ("node_evals", C.c_uint64), ("device_ms", C.c_double)]
+                ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
+                ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_activations", C.c_uint64),
+                ("launches", C.c_uint64)]
 
 
 _lib = None
@@ -78,8 +80,12 @@ def load():
                                      C.POINTER(eik_stats)]
         L.eik_gradient.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, C.c_int32,
                                    C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
+        L.eik_gradient_device.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, C.c_int32,
+                                          C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
+        L.eik_ctx_stream.argtypes = [P]
+        L.eik_ctx_stream.restype = C.c_void_p
         for f in ("eik_ctx_create", "eik_ctx_destroy", "eik_model_upload", "eik_model_upload_device",
-                  "eik_model_release", "eik_traveltime", "eik_gradient"):
+                  "eik_model_release", "eik_traveltime", "eik_gradient", "eik_gradient_device"):
             getattr(L, f).restype = C.c_int
         _lib = L
         return L

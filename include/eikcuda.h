@@ -96,6 +96,11 @@ typedef struct {
   uint64_t tile_activations; /* coarse tiles processed */
   uint64_t node_evals;       /* coarse node updates evaluated */
   double device_ms;          /* device time of the call (CUDA events) */
+  double fine_ms;            /* start-up stage: refined-grid FMM or source box (CUDA events) */
+  double solve_ms;           /* coarse forward solve kernel (CUDA events) */
+  double adj_ms;             /* adjoint dataflow solve kernel (CUDA events) */
+  uint64_t adj_activations;  /* adjoint tiles processed */
+  uint64_t launches;         /* kernels this call launched */
 } eik_stats;
 
 /* Fills the reference defaults of ExtraParams(). */
@@ -106,6 +111,9 @@ void eik_extra_defaults(eik_extra* ep);
 int eik_ctx_create(int device, size_t hbm_budget, eik_ctx** out);
 int eik_ctx_destroy(eik_ctx* ctx);
 const char* eik_last_error(eik_ctx* ctx);
+/* The CUDA stream (cudaStream_t) all work of this context runs on, for callers that order
+ * their own work or events against it. */
+void* eik_ctx_stream(eik_ctx* ctx);
 
 /* Uploads a velocity model (host, column-major, FP64) and keeps it resident. Checks
  * all(vel.>0) (eikmainfwd.jl:45). */
@@ -127,6 +135,15 @@ int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* c
                  const int64_t* rec_off, const double* rec, const double* pickobs,
                  const double* stdobs, int32_t whichgrad, const eik_extra* ep, double* gradvel,
                  double* gradsrc, double* misfit, eik_stats* stats);
+
+/* Same as eik_gradient with inputs and outputs in this context's device memory (for callers
+ * that keep observations and results on the GPU: autodiff wrappers, serving). rec_off stays
+ * on the host. gradvel_dev: N values, gradsrc_dev: nsrc x ndim, misfit_dev: 1 value; each
+ * nullable. Returns when the results are written. */
+int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc_dev,
+                        const int64_t* rec_off, const double* rec_dev, const double* pickobs_dev,
+                        const double* stdobs_dev, int32_t whichgrad, const eik_extra* ep,
+                        double* gradvel_dev, double* gradsrc_dev, double* misfit_dev, eik_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -3,6 +3,8 @@ declared in include/eikcuda.h (no compute call: there may be no GPU here)."""
 import ctypes as C
 import os
 import re
+import shutil
+import subprocess
 
 import pytest
 
@@ -27,10 +29,29 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
-def test_struct_sizes_match_header():
-    assert C.sizeof(_lib.eik_grid) == 4 + 4 + 3 * 8 + 3 * 8 + 3 * 8
-    assert C.sizeof(_lib.eik_extra) == 8 * 4
-    assert C.sizeof(_lib.eik_stats) == 4 + 4 + 8 + 8 + 8
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and offsetof of a header struct, from a C compiler."""
+    prog = tmp_path / "layout.c"
+    lines = [f'printf("%zu\\n", sizeof({struct}));']
+    lines += [f'printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    prog.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "eikcuda.h"\n'
+                    "int main(void) {" + "".join(lines) + " return 0; }\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(REPO, "include"), str(prog), "-o", str(exe)],
+                   check=True)
+    out = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    return out[0], out[1:]
+
+
+@pytest.mark.parametrize("name", ["eik_grid", "eik_extra", "eik_stats"])
+def test_struct_layouts_match_header(tmp_path, name):
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    cls = getattr(_lib, name)
+    fields = [f[0] for f in cls._fields_]
+    size, offs = _c_layout(tmp_path, name, fields)
+    assert C.sizeof(cls) == size
+    assert [getattr(cls, f).offset for f in fields] == offs
 
 
 def test_extra_defaults_match_reference():
