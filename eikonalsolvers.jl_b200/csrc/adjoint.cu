@@ -381,7 +381,7 @@ __device__ int adj_process_tile(const AdjArgs& aa, AdjSmem<ND>& S, int prob, lon
     tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
   }
   // reverse-time priority: later traveltimes first
-  *prio_out = fmax(0.0, 1.0 / P.tinv * (double)QBUCKETS - tmin);
+  *prio_out = fmax(0.0, (double)QBUCKETS / P.tinv - tmin);
   return fm;
 }
 
@@ -456,14 +456,38 @@ __global__ void __launch_bounds__(ADJ_THREADS) adj_solve_kernel(AdjArgs aa) {
   }
 }
 
-// Every tile starts queued (bucket by reverse time of its latest node is refined by the
-// dataflow itself); a tile without a ready node returns at once.
-__global__ void adj_seed_kernel(SolveArgs a, int nprob) {
-  const CoarseProblem& P0 = a.probs[0];
-  const long long tp = (long long)P0.nt[0] * P0.nt[1] * P0.nt[2];  // every problem has the same grid
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.ntiles; q += (long long)gridDim.x * blockDim.x) {
-    const int prob = (int)(q / tp);
-    enqueue_tile(a, prob, q - (long long)prob * tp, FACES_ALL, 0.0);
+// The dataflow starts from the nodes no stencil depends on (the late ends of the
+// characteristics: local maxima of t); their tiles are queued, latest times first.
+template <int ND>
+__global__ void adj_roots_kernel(SolveArgs a, long long N) {
+  using Cfg = TileCfg<ND>;
+  const long long tot = N * a.nprob;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(q / N);
+    const long long l = q - (long long)s * N;
+    const CoarseProblem& P = a.probs[s];
+    const GridDesc& g = P.g;
+    if (is_source(P, l)) continue;
+    const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
+    bool root = true;
+    for (int ax = 0; ax < ND && root; ax++)
+      for (int dl = -2; dl <= 2 && root; dl++) {
+        if (dl == 0) continue;
+        int pr[3] = {c[0], c[1], c[2]};
+        pr[ax] += dl;
+        if (pr[ax] < 0 || pr[ax] >= g.n[ax]) continue;
+        int8_t cd[3];
+        unpack_codes(P.code[lin3(g, pr[0], pr[1], pr[2])], cd);
+        const int cc = cd[ax];
+        if (cc == 0) continue;
+        const int ac = cc < 0 ? -cc : cc;
+        const int p = -dl * (cc > 0 ? -1 : 1);
+        if (p >= 1 && p <= ac) root = false;
+      }
+    if (!root) continue;
+    const long long tile = (long long)(c[0] / Cfg::TX) +
+                           (long long)P.nt[0] * ((long long)(c[1] / Cfg::TY) + (long long)P.nt[1] * (c[2] / Cfg::TZ));
+    enqueue_tile(a, s, tile, FACES_ALL, fmax(0.0, (double)QBUCKETS / P.tinv - P.t[l]));
   }
 }
 
@@ -1129,7 +1153,8 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   aa.sa.activations = fw.sa.activations + 4;  // own counters; the forward's stay readable
   aa.sa.node_evals = fw.sa.activations + 5;
   launch_queue_init(aa.sa, st);
-  adj_seed_kernel<<<ctx->nsm * 4, 256, 0, st>>>(aa.sa, (int)nsrc);
+  if (nd == 3) adj_roots_kernel<3><<<ctx->nsm * 8, 256, 0, st>>>(aa.sa, N);
+  else adj_roots_kernel<2><<<ctx->nsm * 8, 256, 0, st>>>(aa.sa, N);
   cudaEventRecord(ctx->evk[4], st);
   if (nd == 3) launch_adj_solve<3>(aa, ctx->nsm, st);
   else launch_adj_solve<2>(aa, ctx->nsm, st);
