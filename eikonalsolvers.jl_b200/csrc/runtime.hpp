@@ -55,6 +55,7 @@ struct ForwardState {
 };
 
 int fail(eik_ctx* ctx, int code, const char* fmt, ...);
+int make_griddesc(eik_ctx* ctx, const eik_grid* g, GridDesc* out);
 int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const eik_extra& ep,
                    ForwardState* fw, eik_stats* stats);
 int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats);

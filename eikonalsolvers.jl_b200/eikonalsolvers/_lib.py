@@ -21,7 +21,7 @@ ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EI
 
 EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last_error",
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
-            "eik_gradient", "eik_gradient_device", "eik_ctx_stream"]
+            "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc"]
 
 
 class EikError(RuntimeError):
@@ -82,6 +82,8 @@ def load():
                                    C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
         L.eik_gradient_device.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, C.c_int32,
                                           C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
+        L.eik_ttimemisfit_noalloc.argtypes = [C.POINTER(eik_grid), C.c_int64, P, P, P, P, P, P, P]
+        L.eik_ttimemisfit_noalloc.restype = C.c_int
         L.eik_ctx_stream.argtypes = [P]
         L.eik_ctx_stream.restype = C.c_void_p
         for f in ("eik_ctx_create", "eik_ctx_destroy", "eik_model_upload", "eik_model_upload_device",

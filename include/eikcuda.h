@@ -145,6 +145,21 @@ int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const do
                         const double* stdobs_dev, int32_t whichgrad, const eik_extra* ep,
                         double* gradvel_dev, double* gradsrc_dev, double* misfit_dev, eik_stats* stats);
 
+/* No counterpart in the reference. Misfit 0.5*Σ_s Σ_r (t - obs)²/σ² of nsrc traveltime
+ * grids that are already in device memory (ttgrids_dev: nsrc x N, as eik_traveltime
+ * returns them), with receivers, observations and the result also in device memory and
+ * rec_off on the host. It allocates no device memory: for callers that may not call
+ * cudaMalloc (a framework op under the framework's own allocator, a sampler callback that
+ * must not change the device's memory map). Its scratch is a fixed ~1 MB array in the
+ * library, so nsrc is limited to 65536 (larger calls fail with EIK_ERR_OUT_OF_BUDGET).
+ * All calls on a device share that array: calls that overlap on the GPU race, so
+ * serialise them. The first call on each device looks up the array's address; make that
+ * first call before any stream capture. Runs on `stream` (a cudaStream_t; NULL = legacy
+ * default stream) and returns when the result is written. */
+int eik_ttimemisfit_noalloc(const eik_grid* grd, int64_t nsrc, const double* ttgrids_dev,
+                            const int64_t* rec_off, const double* rec_dev, const double* pickobs_dev,
+                            const double* stdobs_dev, double* misfit_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
