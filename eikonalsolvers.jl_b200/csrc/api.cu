@@ -143,15 +143,18 @@ int check_extra(eik_ctx* ctx, const eik_extra* ep) {
   return EIK_OK;
 }
 
-__global__ void slowness_kernel(const double* vel, double* slow, long long n, int* nonpos, double* ssum) {
-  double acc = 0.0;
+__global__ void slowness_kernel(const double* vel, double* slow, long long n, int* nonpos, double* ssum,
+                                unsigned long long* smin) {
+  double acc = 0.0, mn = EIK_INF;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const double v = vel[i];
     if (!(v > 0.0)) atomicExch(nonpos, 1);
     slow[i] = 1.0 / v;
     acc += (v > 0.0) ? 1.0 / v : 0.0;
+    if (v > 0.0) mn = fmin(mn, 1.0 / v);
   }
   atomicAdd(ssum, acc);
+  atomicMin(smin, (unsigned long long)__double_as_longlong(mn));  // positive doubles order as integers
 }
 
 int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev, eik_model_id* out) {
@@ -169,14 +172,17 @@ int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev,
   if (dev) CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   else CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyHostToDevice, ctx->stream));
   int* dflag = nullptr;
-  CUDA_OK(ctx, cudaMalloc(&dflag, 2 * sizeof(double)));
+  CUDA_OK(ctx, cudaMalloc(&dflag, 3 * sizeof(double)));
   CUDA_OK(ctx, cudaMemsetAsync(dflag, 0, 2 * sizeof(double), ctx->stream));
+  CUDA_OK(ctx, cudaMemsetAsync(reinterpret_cast<double*>(dflag) + 2, 0x7f, sizeof(double), ctx->stream));
   double* dsum = reinterpret_cast<double*>(dflag) + 1;
-  slowness_kernel<<<592, 256, 0, ctx->stream>>>(m.vel, m.slow, m.N, dflag, dsum);
+  unsigned long long* dmin = reinterpret_cast<unsigned long long*>(dflag) + 2;
+  slowness_kernel<<<592, 256, 0, ctx->stream>>>(m.vel, m.slow, m.N, dflag, dsum, dmin);
   int nonpos = 0;
   double ssum = 0.0;
   CUDA_OK(ctx, cudaMemcpyAsync(&nonpos, dflag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_OK(ctx, cudaMemcpyAsync(&ssum, dsum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_OK(ctx, cudaMemcpyAsync(&m.smin, dmin, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
   cudaFree(dflag);
   {
@@ -289,6 +295,14 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     P.nt[2] = nt[2];
     P.tbase = s * tiles_per;
     P.tinv = (double)QBUCKETS / m.tscale;
+    {
+      // about one node's traveltime at the largest velocity
+      double dh[3];
+      node_dh(g, 0, dh);
+      double hmin = dh[0];
+      for (int a = 1; a < g.nd; a++) hmin = std::min(hmin, dh[a]);
+      P.delta = ctx->round_gate * hmin * m.smin;
+    }
   }
   CoarseProblem* dp;
   GET(dp, CoarseProblem, "probs", nsrc);
@@ -315,6 +329,23 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   sa.node_evals = ctr + 2 * QBUCKETS + 1;
   sa.pending = (int32_t*)(ctr + 2 * QBUCKETS + 2);
   sa.abort_flag = (int32_t*)(ctr + 2 * QBUCKETS + 3);
+  if ((unsigned long long)nsrc * (unsigned long long)N >= (1ull << 32))
+    return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "more than 2^32 node-sources in one call: split the sources");
+  GET(sa.rs.stamp, int32_t, "rs_stamp", nsrc * N);
+  GET(sa.rs.tent, double, "rs_tent", nsrc * N);
+  GET(sa.rs.dirty, uint8_t, "rs_dirty", nsrc * N);
+  GET(sa.rs.list[0], unsigned int, "rs_list0", nsrc * N);
+  GET(sa.rs.list[1], unsigned int, "rs_list1", nsrc * N);
+  GET(sa.rs.nextmin, unsigned long long, "rs_nextmin", 3 * nsrc);
+  {
+    unsigned int* rc32;
+    GET(rc32, unsigned int, "rs_ctr", 16);
+    sa.rs.cnt = rc32;
+    sa.rs.grab = rc32 + 3;
+    sa.rs.bar = rc32 + 6;
+    sa.rs.rounds = (int32_t*)(rc32 + 8);
+  }
+  sa.rs.max_rounds = 1 << 24;
   sa.err = fb.err;
   sa.probs = dp;
   sa.max_activations = 400ull * (unsigned long long)sa.ntiles + 100000ull;
@@ -333,7 +364,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
   CUDA_OK(ctx, cudaGetLastError());
   cudaEventRecord(ctx->evk[2], st);
-  launch_coarse_solve(sa, ctx->nsm, st);
+  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->nsm, st));
   cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
   fw->fb = fb;
@@ -351,7 +382,9 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
 int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
   unsigned long long ctr[4] = {0, 0, 0, 0};
   uint32_t e = 0;
+  int32_t rounds = 0;
   cudaMemcpyAsync(ctr + 2, fw->sa.activations, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(&rounds, fw->sa.rs.rounds, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
   cudaMemcpyAsync(&e, fw->fb.err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream);
   std::vector<SrcOut> outs(fw->nsrc);
   cudaMemcpyAsync(outs.data(), fw->fb.out, sizeof(SrcOut) * fw->nsrc, cudaMemcpyDeviceToHost, ctx->stream);
@@ -363,6 +396,7 @@ int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
     stats->err_mask |= e;
     stats->tile_activations += ctr[2];
     stats->node_evals += ctr[3];
+    stats->fwd_rounds += (uint64_t)rounds;
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, ctx->evk[0], ctx->evk[1]);
     cudaEventElapsedTime(&b, ctx->evk[2], ctx->evk[3]);
@@ -433,6 +467,17 @@ int eik_ctx_destroy(eik_ctx* ctx) {
 }
 
 void* eik_ctx_stream(eik_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
+  if (!ctx || !name) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (std::strcmp(name, "round_gate") == 0) {
+    if (!(value > 0.0 && value < 1e6)) return fail(ctx, EIK_ERR_ASSERT, "round_gate must be in (0, 1e6)");
+    ctx->round_gate = value;
+    return EIK_OK;
+  }
+  return fail(ctx, EIK_ERR_ASSERT, "unknown parameter '%s'", name);
+}
 
 const char* eik_last_error(eik_ctx* ctx) {
   (void)ctx;

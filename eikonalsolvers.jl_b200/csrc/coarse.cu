@@ -1,19 +1,29 @@
 // Coarse-grid forward solve: the reference's heap-ordered FMM main loop
 // (ttFMM_core!, src/EikSolv/eikmainfwd.jl:427-823) restated as the fixed point of the
-// order rule of stencil.cuh and solved by a block-tiled active-list iteration.
+// order rule of stencil.cuh and solved by a block-tiled active-node iteration.
 //
-// One persistent launch serves many problems (sources, possibly of different grids)
-// through one queue of tiles. A CTA takes a tile, stages its traveltimes and keys plus a
-// 2-node halo in shared memory, iterates the rule on its active nodes until nothing
-// changes (or a pass limit), writes the changed nodes back and queues the neighbouring
-// tiles whose halo it changed. The launch ends when no tile is queued or in work.
-// Every wait is bounded (global timer), every solve bounded in tile activations; both
-// report through an error word instead of trapping.
+// One cooperative persistent launch serves many problems (sources, possibly of different
+// grids). It runs in rounds separated by a grid barrier. In round r each listed tile is
+// taken by one warp, which stages its traveltimes and keys plus a 2-node halo in shared
+// memory, evaluates its active nodes whose potential is below the problem's threshold
+// until nothing below it changes, writes the changed nodes back and marks the nodes of
+// the neighbouring tiles that read them for the next round. The threshold follows the
+// front (smallest pending potential + about one node's traveltime), so the rounds sweep
+// the grid in traveltime order. Every wait is bounded (global timer), the number of rounds
+// is bounded; both report through an error word instead of trapping.
 #include "kernels.cuh"
 #include "queue.cuh"
 
 namespace eik {
 
+
+// Lists node gid (problem * N + node) for round r, once per round.
+__device__ __forceinline__ void list_node(const SolveArgs& a, int r, unsigned int gid) {
+  if (atomicExch(a.rs.stamp + gid, r) != r) {
+    const unsigned int i = atomicAdd(a.rs.cnt + (r % 3), 1u);
+    a.rs.list[r & 1][i] = gid;
+  }
+}
 
 // ----------------------------------------------------------------------- init --
 __global__ void coarse_init_kernel(const CoarseProblem* probs, int nprob, long long N) {
@@ -50,14 +60,35 @@ __global__ void queue_init_kernel(SolveArgs a) {
   }
 }
 
-template <int ND>
-__device__ __forceinline__ long long tile_of(const CoarseProblem& P, int i, int j, int k) {
-  using C = TileCfg<ND>;
-  return (long long)(i / C::TX) + (long long)P.nt[0] * ((long long)(j / C::TY) + (long long)P.nt[1] * (k / C::TZ));
+
+__global__ void rounds_init_kernel(SolveArgs a) {
+  const long long tot = npts(a.probs[0].g) * a.nprob;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * blockDim.x) {
+    a.rs.stamp[q] = -1;
+    a.rs.dirty[q] = 1;
+  }
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < 3LL * a.nprob;
+       q += (long long)gridDim.x * blockDim.x)
+    a.rs.nextmin[q] = (unsigned long long)__double_as_longlong(EIK_INF);
+  if (blockIdx.x == 0 && threadIdx.x < 3) {
+    a.rs.cnt[threadIdx.x] = 0;
+    a.rs.grab[threadIdx.x] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.rs.bar[0] = 0;
+    a.rs.bar[1] = 0;
+    *a.rs.rounds = 0;
+    *a.pending = 0;
+    *a.activations = 0;
+    *a.node_evals = 0;
+    *a.abort_flag = 0;
+  }
 }
 
 // Seeds: fixed traveltimes of the source points (coarse source box or coarse-coincident
-// accepted fine nodes); the tiles within two nodes of a seed start the solve.
+// accepted fine nodes); the tiles within two nodes of a seed start round 0, whose
+// threshold is based on the smallest seed traveltime.
 template <int ND>
 __global__ void seed_kernel(SolveArgs a, ForwardBatch fb) {
   const int s = blockIdx.x;
@@ -78,115 +109,35 @@ __global__ void seed_kernel(SolveArgs a, ForwardBatch fb) {
     const int j = (int)((l / P.g.n[0]) % P.g.n[1]);
     const int k = (int)(l / ((long long)P.g.n[0] * P.g.n[1]));
     const int c[3] = {i, j, k};
-    const double pr = fb.seed_tt[(size_t)s * fb.seedcap + q];
-    enqueue_tile(a, s, tile_of<ND>(P, i, j, k), FACES_ALL, pr);
+    const double tt = fb.seed_tt[(size_t)s * fb.seedcap + q];
+    if (tt < EIK_INF) atomicMin(a.rs.nextmin + s, (unsigned long long)__double_as_longlong(tt));
+    const unsigned long long gbase = (unsigned long long)s * (unsigned long long)npts(P.g);
     for (int ax = 0; ax < ND; ax++)
-      for (int d = -2; d <= 2; d += 4) {
+      for (int d = -2; d <= 2; d++) {
+        if (d == 0) continue;
         int p[3] = {c[0], c[1], c[2]};
         p[ax] += d;
         if (p[ax] < 0 || p[ax] >= P.g.n[ax]) continue;
-        enqueue_tile(a, s, tile_of<ND>(P, p[0], p[1], p[2]), FACES_ALL, pr);
+        list_node(a, 0, (unsigned int)(gbase + lin3(P.g, p[0], p[1], p[2])));
       }
   }
 }
 
-// ------------------------------------------------------------------ tile solve --
-// One warp owns one tile at a time (its own shared-memory slice, warp-level syncs only),
-// so an SM keeps many independent tiles in flight and hides the FP64 latency of the
-// update; CTAs only group warps for occupancy.
-template <int ND>
-struct TileSmem {
-  using C = TileCfg<ND>;
-  static constexpr int TN = C::TX * C::TY * C::TZ;
-  static constexpr int HN = C::HX * C::HY * C::HZ;
-  double t[HN];
-  double L[HN];       // key level of special nodes
-  double slow[TN];
-  uint8_t fl[HN];     // bit0 special key, bits 1..4 depth
-  uint8_t code[TN];
-  uint8_t act[TN];    // to be evaluated (plain stores of 1 from any lane)
-  uint8_t dirty[TN];  // changed, to be written back
-  int16_t list[TN];
-};
-
-template <int ND>
-__device__ __forceinline__ int hidx(int x, int y, int z) {
-  using C = TileCfg<ND>;
-  return (x + C::H) + C::HX * ((y + C::H) + C::HY * (ND == 3 ? z + C::H : 0));
-}
-
-template <int ND>
-__device__ __forceinline__ void smem_keyLd(const TileSmem<ND>& S, int h, double* L, int* d) {
-  const uint8_t f = S.fl[h];
-  if (f & 1) {
-    *L = S.L[h];
-    *d = f >> 1;
+// ------------------------------------------------------------------ node solve --
+// Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise.
+__device__ __forceinline__ void node_key(const CoarseProblem& P, long long l, double t, uint8_t cb, double* L, int* d) {
+  if (cb & CODE_SRC_BIT) {
+    *L = __ldcg(P.kL + l);
+    *d = __ldcg(P.kd + l);
   } else {
-    *L = S.t[h];
+    *L = t;
     *d = 0;
   }
 }
 
-// Smallest traveltime among the in-grid immediate neighbours of tile node li.
-template <int ND>
-__device__ __forceinline__ double node_potential(const TileSmem<ND>& S, const GridDesc& g, int ox, int oy,
-                                                 int oz, int li) {
-  using C = TileCfg<ND>;
-  const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-  const int c[3] = {ox + x, oy + y, oz + z};
-  const int hc[3] = {x, y, z};
-  double pm = EIK_INF;
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int sh = -1; sh <= 1; sh += 2) {
-      if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
-      int q[3] = {hc[0], hc[1], hc[2]};
-      q[ax] += sh;
-      pm = fmin(pm, S.t[hidx<ND>(q[0], q[1], q[2])]);
-    }
-  return pm;
-}
-
-template <int ND>
-__device__ __forceinline__ double eval_node(const TileSmem<ND>& S, const GridDesc& g, int ox, int oy, int oz,
-                                            int li, int8_t* cd, Key* kk, bool* neg) {
-  using C = TileCfg<ND>;
-  const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-  const int c[3] = {ox + x, oy + y, oz + z};
-  const int hc[3] = {x, y, z};
-  Nbhd nb;
-  nb_clear(nb);
-  node_dh(g, c[0], nb.dh);
-  nb.slow = S.slow[li];
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int l = 0; l < 2; l++) {
-      const int sh = l == 0 ? 1 : -1;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += sh;
-      if (p[ax] < 0 || p[ax] >= g.n[ax]) continue;
-      int q[3] = {hc[0], hc[1], hc[2]};
-      q[ax] += sh;
-      const int h1 = hidx<ND>(q[0], q[1], q[2]);
-      double L;
-      int d;
-      smem_keyLd<ND>(S, h1, &L, &d);
-      nb_put1(nb, ax, l, S.t[h1], L, d);
-      bool ok = true;
-#pragma unroll
-      for (int dd = 0; dd < ND; dd++)
-        if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
-      if (ok) {
-        q[ax] += sh;
-        const int h2 = hidx<ND>(q[0], q[1], q[2]);
-        smem_keyLd<ND>(S, h2, &L, &d);
-        nb_put2(nb, ax, l, S.t[h2], L, d);
-      }
-    }
-  return prefix_rule<ND>(nb, cd, kk, neg);
-}
+// Neighbour directions of a node: k = 4*axis + {0: -2, 1: -1, 2: +1, 3: +2}; bit 12 = itself.
+constexpr int DIR_SELF = 12;
+__device__ __forceinline__ int dir_off(int k) { return (k & 3) < 2 ? (k & 3) - 2 : (k & 3) - 1; }
 
 __device__ __forceinline__ double warp_min(double v) {
 #pragma unroll
@@ -194,290 +145,292 @@ __device__ __forceinline__ double warp_min(double v) {
   return v;
 }
 
-// Processes one tile with the 32 lanes of the calling warp. Returns the dirty-face mask
-// (bit 6: not converged within the pass limit) and the smallest changed face traveltime.
-template <int ND>
-__device__ int process_tile(const SolveArgs& a, TileSmem<ND>& S, int prob, long long tile, uint32_t faces,
-                            double* fmin_out) {
-  using C = TileCfg<ND>;
-  constexpr int TN = TileSmem<ND>::TN, HN = TileSmem<ND>::HN;
-  constexpr int NPT = (TN + 31) / 32;
-  const CoarseProblem& P = a.probs[prob];
-  const GridDesc& g = P.g;
-  const int tx = (int)(tile % P.nt[0]);
-  const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
-  const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
-  const int ox = tx * C::TX, oy = ty * C::TY, oz = tz * C::TZ;
-  const int lane = threadIdx.x & 31;
-
-  // ---- stage tile + halo
-  for (int h = lane; h < HN; h += 32) {
-    const int hx = h % C::HX, hy = (h / C::HX) % C::HY, hz = h / (C::HX * C::HY);
-    const int gx = ox + hx - C::H, gy = oy + hy - C::H, gz = (ND == 3) ? oz + hz - C::H : 0;
-    double tv = EIK_INF, Lv = 0.0;
-    uint8_t f = 0;
-    if (gx >= 0 && gx < g.n[0] && gy >= 0 && gy < g.n[1] && gz >= 0 && gz < g.n[2]) {
-      const long long l = lin3(g, gx, gy, gz);
-      // L2-coherent loads: other SMs write these between activations of this tile
-      tv = __ldcg(P.t + l);
-      const uint8_t cb = __ldcg(P.code + l);
-      if (cb & CODE_SRC_BIT) {
-        Lv = __ldcg(P.kL + l);
-        f = (uint8_t)(1 | (__ldcg(P.kd + l) << 1));
-      }
-      const bool inter = hx >= C::H && hx < C::H + C::TX && hy >= C::H && hy < C::H + C::TY &&
-                         (ND == 2 || (hz >= C::H && hz < C::H + C::TZ));
-      if (inter) {
-        const int li = (hx - C::H) + C::TX * ((hy - C::H) + C::TY * (ND == 3 ? hz - C::H : 0));
-        S.code[li] = cb & 0x7f;
-        S.slow[li] = P.slow[l];
-      }
-    }
-    S.t[h] = tv;
-    S.L[h] = Lv;
-    S.fl[h] = f;
-  }
-  __syncwarp();
-  // ---- initial active set from the dirty faces (source points are never updated)
-#pragma unroll
-  for (int r = 0; r < NPT; r++) {
-    const int li = lane + 32 * r;
-    if (li >= TN) continue;
-    const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-    bool act = (faces & FACES_ALL) != 0;
-    act = act || ((faces & 1) && x < 2) || ((faces & 2) && x >= C::TX - 2) || ((faces & 4) && y < 2) ||
-          ((faces & 8) && y >= C::TY - 2) || ((faces & 16) && z < 2) || ((faces & 32) && z >= C::TZ - 2);
-    const int h = hidx<ND>(x, y, z);
-    const bool src = (S.fl[h] & 1) && S.L[h] == -EIK_INF;
-    const bool inside = ox + x < g.n[0] && oy + y < g.n[1] && oz + z < g.n[2];
-    S.act[li] = (act && !src && inside) ? 1 : 0;
-    S.dirty[li] = 0;
-  }
-  double hmin = g.spac[0];
-  if (!is_cart(g)) {
-    double dh[3];
-    node_dh(g, 0, dh);
-    hmin = fmin(dh[0], dh[1]);
-    if (ND == 3) hmin = fmin(hmin, dh[2]);
-  }
-  const double gate = a.gate * hmin;
-  __syncwarp();
-
-  int fm = 0;
-  double fmin_changed = EIK_INF;
-  int pass = 0;
-  unsigned long long evals = 0;
-  bool unconv = false;
-  for (;;) {
-    // ---- front of the active nodes, gated evaluation list
-    double pot[NPT];
-    double mypot = EIK_INF;
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      const int li = lane + 32 * r;
-      pot[r] = EIK_INF;
-      if (li >= TN || !S.act[li]) continue;
-      pot[r] = node_potential<ND>(S, g, ox, oy, oz, li);
-      if (!(pot[r] < EIK_INF)) S.act[li] = 0;  // no reached neighbour: nothing to compute
-      mypot = fmin(mypot, pot[r]);
-    }
-    const double front = warp_min(mypot);
-    if (!(front < EIK_INF)) break;
-    int nlist = 0;
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      const int li = lane + 32 * r;
-      const bool sel = li < TN && S.act[li] && pot[r] <= front + gate * S.slow[li];
-      const unsigned m = __ballot_sync(0xffffffffu, sel);
-      if (sel) {
-        S.list[nlist + __popc(m & ((1u << lane) - 1u))] = (int16_t)li;
-        S.act[li] = 0;
-      }
-      nlist += __popc(m);
-    }
-    __syncwarp();
-    // ---- evaluate
-    double nv[NPT];
-    Key nk[NPT];
-    uint8_t nc[NPT];
-    int nli[NPT];
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      const int e = lane + 32 * r;
-      nli[r] = -1;
-      if (e >= nlist) continue;
-      const int li = S.list[e];
-      int8_t cd[3] = {0, 0, 0};
-      bool neg = false;
-      nv[r] = eval_node<ND>(S, g, ox, oy, oz, li, cd, &nk[r], &neg);
-      nc[r] = pack_codes(cd, ND);
-      nli[r] = li;
-      evals++;
-    }
-    __syncwarp();
-    // ---- apply
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      const int li = nli[r];
-      if (li < 0) continue;
-      const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-      const int hm = hidx<ND>(x, y, z);
-      double Lo;
-      int dold;
-      smem_keyLd<ND>(S, hm, &Lo, &dold);
-      const double ot = S.t[hm];
-      const Key old = Key{Lo, dold, ot};
-      const bool same_t = (nv[r] == ot) || (isinf(nv[r]) && isinf(ot));
-      const bool tkchange = !(same_t && key_eq(nk[r], old));
-      if (!tkchange && nc[r] == S.code[li]) continue;
-      S.code[li] = nc[r];
-      S.dirty[li] = 1;
-      if (!tkchange) continue;
-      S.t[hm] = nv[r];
-      const bool special = !(nk[r].L == nv[r] && nk[r].d == 0);
-      S.fl[hm] = special ? (uint8_t)(1 | (nk[r].d << 1)) : (uint8_t)0;
-      S.L[hm] = special ? nk[r].L : 0.0;
-      const int xyz[3] = {x, y, z};
-      const int T3[3] = {C::TX, C::TY, C::TZ};
-      const int o3[3] = {ox, oy, oz};
-#pragma unroll
-      for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-        for (int d = -2; d <= 2; d++) {
-          if (d == 0) continue;
-          int q[3] = {xyz[0], xyz[1], xyz[2]};
-          q[ax] += d;
-          if (q[ax] < 0 || q[ax] >= T3[ax] || o3[ax] + q[ax] >= g.n[ax]) continue;
-          const int lq = q[0] + C::TX * (q[1] + C::TY * q[2]);
-          const int hq = hidx<ND>(q[0], q[1], q[2]);
-          const bool src = (S.fl[hq] & 1) && S.L[hq] == -EIK_INF;
-          if (!src) S.act[lq] = 1;
-        }
-      int f = 0;
-      if (x < 2) f |= 1;
-      if (x >= C::TX - 2) f |= 2;
-      if (y < 2) f |= 4;
-      if (y >= C::TY - 2) f |= 8;
-      if (ND == 3 && z < 2) f |= 16;
-      if (ND == 3 && z >= C::TZ - 2) f |= 32;
-      if (f) {
-        fm |= f;
-        fmin_changed = fmin(fmin_changed, nv[r]);
-      }
-    }
-    __syncwarp();
-    pass++;
-    bool anyact = false;
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      const int li = lane + 32 * r;
-      anyact = anyact || (li < TN && S.act[li]);
-    }
-    if (!__any_sync(0xffffffffu, anyact)) break;
-    if (pass >= a.max_passes) {
-      unconv = true;
-      break;
-    }
-  }
-  // ---- write back
-#pragma unroll
-  for (int r = 0; r < NPT; r++) {
-    const int li = lane + 32 * r;
-    if (li >= TN || !S.dirty[li]) continue;
-    const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-    const int h = hidx<ND>(x, y, z);
-    const long long l = lin3(g, ox + x, oy + y, oz + z);
-    P.t[l] = S.t[h];
-    const bool special = S.fl[h] & 1;
-    P.code[l] = (uint8_t)(S.code[li] | (special ? CODE_SRC_BIT : 0));
-    if (special) {
-      P.kL[l] = S.L[h];
-      P.kd[l] = (uint8_t)(S.fl[h] >> 1);
-    }
-  }
-  // reduce face mask and trigger time over the warp
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) fm |= __shfl_xor_sync(0xffffffffu, fm, o);
-  *fmin_out = warp_min(fmin_changed);
-  unsigned long long ev = evals;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
-  if (lane == 0 && ev) atomicAdd(a.node_evals, ev);
-  return fm | (unconv ? 64 : 0);
+__device__ __forceinline__ void atomic_min_pos(unsigned long long* p, double v) {
+  // traveltimes and potentials are >= 0: their bit patterns order as the values
+  if (v < EIK_INF && v < __longlong_as_double((long long)ld_volatile(p)))
+    atomicMin(p, (unsigned long long)__double_as_longlong(v));
 }
 
-template <int ND>
-__global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_solve_kernel(SolveArgs a) {
-  extern __shared__ __align__(16) unsigned char solve_smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  TileSmem<ND>& S = reinterpret_cast<TileSmem<ND>*>(solve_smem)[warp];
-  long long idle_since = -1;
-  for (;;) {
-    int ab = (lane == 0) ? *(volatile int*)a.abort_flag : 0;
-    if (__shfl_sync(0xffffffffu, ab, 0)) break;
-    unsigned long long its[QCLAIM] = {0, 0, 0, 0};
-    const int ngot = q_pop_warp(a, its);
-    if (!ngot) {
-      int done = (lane == 0) ? (*(volatile int*)a.pending == 0) : 0;
-      if (__shfl_sync(0xffffffffu, done, 0)) break;
-      if (lane == 0) {
-        const long long now = gtimer_ns();
-        if (idle_since < 0) idle_since = now;
-        if (now - idle_since > a.timeout_ns) {
+// Grid-wide barrier of the cooperative solve launch (all CTAs co-resident). The wait is
+// bounded by the global timer; a CTA that gives up raises the abort flag, which releases
+// the others. Returns false when the solve is aborted.
+__device__ bool grid_barrier(const SolveArgs& a) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    volatile unsigned int* gen = a.rs.bar + 1;
+    const unsigned int g0 = *gen;
+    const unsigned int arrived = atomicAdd(a.rs.bar, 1u);
+    bool ok = true;
+    if (arrived == gridDim.x - 1) {
+      atomicExch(a.rs.bar, 0u);
+      __threadfence();
+      atomicAdd(a.rs.bar + 1, 1u);
+    } else {
+      const long long t0 = gtimer_ns();
+      while (*gen == g0) {
+        if (*(volatile int*)a.abort_flag) {
+          ok = false;
+          break;
+        }
+        if (gtimer_ns() - t0 > a.timeout_ns) {
           atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
           atomicExch(a.abort_flag, 1);
+          ok = false;
+          break;
         }
-        __nanosleep(200);
+        __nanosleep(40);
       }
-      __syncwarp();
-      continue;
     }
-    idle_since = -1;
-    for (int j = 0; j < ngot; j++) {
-      const unsigned long long it = its[j];
-      const int prob = (int)(it >> 40);
-      const long long tile = (long long)(it & ((1ull << 40) - 1));
-      const long long gt = a.probs[prob].tbase + tile;
-      uint32_t faces = 0;
-      if (lane == 0) {
-        atomicExch(a.tile_flag + gt, TS_BUSY);
-        faces = atomicExch(a.tile_faces + gt, 0u);
-        atomicExch(a.tile_prio + gt, (unsigned long long)__double_as_longlong(EIK_INF));
-        __threadfence();
-        const unsigned long long na = atomicAdd(a.activations, 1ull);
-        if (na > a.max_activations) {
-          atomicOr(a.err, ERRB_NOT_CONVERGED);
-          atomicExch(a.abort_flag, 1);
-        }
+    __threadfence();
+    s_ok = ok && !*(volatile int*)a.abort_flag;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// One listed node: gate, evaluate, write back. Returns the directions of the nodes to list
+// for the next round (bit DIR_SELF: this node again) and, in *front, the traveltime that
+// bounds their next evaluation from below.
+template <int ND>
+__device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, unsigned long long gbase, long long l,
+                                 double T, int r, double* front, unsigned long long* evals) {
+  const GridDesc& g = P.g;
+  const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
+  // last evaluated value, still valid while nothing the node reads has changed
+  if (!__ldcg(a.rs.dirty + gbase + l)) {
+    const double tv = __ldcg(a.rs.tent + gbase + l);
+    if (tv > T) {
+      *front = tv;
+      return 1u << DIR_SELF;
+    }
+  }
+  const uint8_t cb = __ldcg(P.code + l);
+  const double told = __ldcg(P.t + l);
+  double Lold;
+  int dold;
+  node_key(P, l, told, cb, &Lold, &dold);
+  if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) return 0;  // source points are fixed
+  // immediate neighbours: potential (the smallest of their traveltimes)
+  double t1[ND][2];
+  long long l1[ND][2];
+  double pot = EIK_INF;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int sh = s == 0 ? 1 : -1;
+      l1[ax][s] = -1;
+      t1[ax][s] = EIK_INF;
+      if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      l1[ax][s] = lin3(g, p[0], p[1], p[2]);
+      t1[ax][s] = __ldcg(P.t + l1[ax][s]);
+      pot = fmin(pot, t1[ax][s]);
+    }
+  if (!(pot < EIK_INF)) return 0;  // nothing reached around it yet
+  Nbhd nb;
+  nb_clear(nb);
+  node_dh(g, c[0], nb.dh);
+  nb.slow = __ldg(P.slow + l);
+  // Lower bound of the node's value: every term of the local update is at least pot and
+  // the quadratic adds at least (2/3) h s / sqrt(ND) (2nd-order coefficients 9/(4h^2)).
+  // Until the round threshold reaches it the node cannot be final: no evaluation yet.
+  double hmin = nb.dh[0];
+#pragma unroll
+  for (int ax = 1; ax < ND; ax++) hmin = fmin(hmin, nb.dh[ax]);
+  const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * nb.slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
+  if (lb > T) {
+    *front = lb;
+    return 1u << DIR_SELF;
+  }
+  // from here the node is evaluated with the neighbours' current values: a change after
+  // this point marks it dirty again (writers store the value, fence, then the flag)
+  a.rs.dirty[gbase + l] = 0;
+  __threadfence();
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      if (l1[ax][s] < 0) continue;
+      const int sh = s == 0 ? 1 : -1;
+      double L;
+      int d;
+      node_key(P, l1[ax][s], t1[ax][s], __ldcg(P.code + l1[ax][s]), &L, &d);
+      nb_put1(nb, ax, s, t1[ax][s], L, d);
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      bool ok = true;  // isonbord on the first neighbour, in every coordinate (eikutils.jl:129-162)
+#pragma unroll
+      for (int dd = 0; dd < ND; dd++)
+        if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
+      if (ok) {
+        p[ax] += sh;
+        const long long l2 = lin3(g, p[0], p[1], p[2]);
+        const double t2 = __ldcg(P.t + l2);
+        node_key(P, l2, t2, __ldcg(P.code + l2), &L, &d);
+        nb_put2(nb, ax, s, t2, L, d);
       }
-      faces = __shfl_sync(0xffffffffu, faces, 0);
-      double pr;
-      const int fm = process_tile<ND>(a, S, prob, tile, faces, &pr);
-      __threadfence();
-      __syncwarp();
-      if (lane == 0) {
+    }
+  int8_t cd[3] = {0, 0, 0};
+  Key nk;
+  bool neg = false;
+  const double nv = prefix_rule<ND>(nb, cd, &nk, &neg);
+  (*evals)++;
+  const uint8_t nc = pack_codes(cd, ND);
+  const bool same_t = (nv == told) || (isinf(nv) && isinf(told));
+  const bool tkchange = !(same_t && key_eq(nk, Key{Lold, dold, told}));
+  const bool special = !(nk.L == nv && nk.d == 0);
+  const uint8_t ncb = (uint8_t)(nc | (special ? CODE_SRC_BIT : 0));
+  a.rs.tent[gbase + l] = nv;
+  if (!tkchange) {
+    if (ncb != cb) P.code[l] = ncb;
+    return 0;
+  }
+  if (nv > T) {  // not final yet: keep the old value and come back when the front is there
+    *front = nv;
+    return 1u << DIR_SELF;
+  }
+  P.t[l] = nv;
+  P.code[l] = ncb;
+  if (special) {
+    P.kL[l] = nk.L;
+    P.kd[l] = (uint8_t)nk.d;
+  }
+  __threadfence();
+  // The nodes whose stencil reads this one (+-1, +-2 along each axis) are evaluated again,
+  // except those whose stored key is at most both the old and the new key of this node:
+  // the order rule of such a node never accepts this one, nor is its termination test
+  // affected, so its value cannot change. A node listed for the current round may be
+  // under evaluation right now and is always listed again.
+  const Key kold = Key{Lold, dold, told};
+  unsigned dirs = 0;
+#pragma unroll
+  for (int k = 0; k < 4 * ND; k++) {
+    const int ax = k >> 2, off = dir_off(k);
+    if (c[ax] + off < 0 || c[ax] + off >= g.n[ax]) continue;
+    int p[3] = {c[0], c[1], c[2]};
+    p[ax] += off;
+    const long long lj = lin3(g, p[0], p[1], p[2]);
+    if (*(volatile int32_t*)(a.rs.stamp + gbase + lj) < r) {
+      const double tj = __ldcg(P.t + lj);
+      double Lj;
+      int dj;
+      node_key(P, lj, tj, __ldcg(P.code + lj), &Lj, &dj);
+      const Key kj = Key{Lj, dj, tj};
+      if (key_le(kj, kold) && key_le(kj, nk)) continue;
+    }
+    a.rs.dirty[gbase + lj] = 1;
+    dirs |= 1u << k;
+  }
+  *front = nv;
+  return dirs;
+}
+
+// Forward coarse solve in rounds (one cooperative launch for all problems). Round r takes
+// the listed nodes; problem p only evaluates nodes whose potential (smallest neighbouring
+// traveltime) is at most T_p(r) = (smallest pending front of p after round r-1) + delta_p,
+// delta_p being about one node's traveltime at the largest velocity. The rounds thus
+// follow the front like a Dijkstra sweep with buckets one node wide. A node whose value or
+// key changed lists the nodes whose stencil reads it for the next round; a node below the
+// front is listed again. The result is the same fixed point as any other evaluation order.
+template <int ND>
+__global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_rounds_kernel(SolveArgs a) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long N = (unsigned long long)npts(a.probs[0].g);  // every problem has the same grid
+  unsigned long long evals = 0;
+  int r = 0;
+  for (; r < a.rs.max_rounds; r++) {
+    const int b3 = r % 3, nb3 = (r + 1) % 3;
+    const unsigned int n = *(volatile unsigned int*)(a.rs.cnt + b3);
+    if (n == 0) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.activations, (unsigned long long)n);  // list entries
+    const unsigned int* L = a.rs.list[r & 1];
+    unsigned int* Lnext = a.rs.list[(r + 1) & 1];
+    const unsigned long long* nm = a.rs.nextmin + (size_t)b3 * a.nprob;
+    unsigned long long* nmn = a.rs.nextmin + (size_t)nb3 * a.nprob;
+    for (;;) {
+      unsigned int base = 0;
+      if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) break;
+      const unsigned int idx = base + lane;
+      unsigned dirs = 0;
+      double front = EIK_INF;
+      int prob = 0;
+      long long l = 0;
+      if (idx < n) {
+        const unsigned int gid = L[idx];
+        prob = (int)(gid / N);
+        l = (long long)(gid - (unsigned long long)prob * N);
         const CoarseProblem& P = a.probs[prob];
-        const int tx = (int)(tile % P.nt[0]);
-        const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
-        const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
-        auto nbt = [&](int x, int y, int z) { return (long long)x + (long long)P.nt[0] * (y + (long long)P.nt[1] * z); };
-        if ((fm & 1) && tx > 0) enqueue_tile(a, prob, nbt(tx - 1, ty, tz), 2u, pr);
-        if ((fm & 2) && tx + 1 < P.nt[0]) enqueue_tile(a, prob, nbt(tx + 1, ty, tz), 1u, pr);
-        if ((fm & 4) && ty > 0) enqueue_tile(a, prob, nbt(tx, ty - 1, tz), 8u, pr);
-        if ((fm & 8) && ty + 1 < P.nt[1]) enqueue_tile(a, prob, nbt(tx, ty + 1, tz), 4u, pr);
-        if (ND == 3) {
-          if ((fm & 16) && tz > 0) enqueue_tile(a, prob, nbt(tx, ty, tz - 1), 32u, pr);
-          if ((fm & 32) && tz + 1 < P.nt[2]) enqueue_tile(a, prob, nbt(tx, ty, tz + 1), 16u, pr);
-        }
-        if (fm & 64) {
-          atomicOr(a.tile_faces + gt, FACES_ALL);
-          atomicMin(a.tile_prio + gt, (unsigned long long)__double_as_longlong(pr));
-          atomicExch(a.tile_flag + gt, TS_BUSY_DIRTY);
-        }
-        __threadfence();
-        finish_tile(a, prob, tile);
+        const double T = __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta;
+        const unsigned long long gb = (unsigned long long)prob * N;
+        dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals)
+                         : process_node<2>(a, P, gb, l, T, r, &front, &evals);
       }
-      __syncwarp();
+      // list the next round's nodes once each (per-node round stamps)
+      const CoarseProblem& P = a.probs[prob];
+      const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
+                        (int)(l / ((long long)P.g.n[0] * P.g.n[1]))};
+      const unsigned long long gbase = (unsigned long long)prob * N;
+      unsigned keep = 0;
+      for (int k = 0; k <= DIR_SELF; k++) {
+        if (!((dirs >> k) & 1u)) continue;
+        long long nl = l;
+        if (k != DIR_SELF) {
+          int p[3] = {c[0], c[1], c[2]};
+          p[k >> 2] += dir_off(k);
+          nl = lin3(P.g, p[0], p[1], p[2]);
+        }
+        if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
+      }
+      // warp-aggregated append: one atomic per 32 nodes
+      const int cntl = __popc(keep);
+      int incl = cntl;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      unsigned int wbase = 0;
+      if (lane == 0 && total) wbase = atomicAdd(a.rs.cnt + nb3, (unsigned int)total);
+      wbase = __shfl_sync(0xffffffffu, wbase, 0) + (unsigned int)(incl - cntl);
+      for (int k = 0; k <= DIR_SELF; k++) {
+        if (!((keep >> k) & 1u)) continue;
+        long long nl = l;
+        if (k != DIR_SELF) {
+          int p[3] = {c[0], c[1], c[2]};
+          p[k >> 2] += dir_off(k);
+          nl = lin3(P.g, p[0], p[1], p[2]);
+        }
+        Lnext[wbase++] = (unsigned int)(gbase + nl);
+      }
+      if (keep) atomic_min_pos(nmn + prob, front);
+    }
+    // buffers of round r+2 (last used in round r-1)
+    if (blockIdx.x == 0) {
+      const int c3 = (r + 2) % 3;
+      if (threadIdx.x == 0) {
+        a.rs.cnt[c3] = 0;
+        a.rs.grab[c3] = 0;
+      }
+      for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
+        a.rs.nextmin[(size_t)c3 * a.nprob + p] = (unsigned long long)__double_as_longlong(EIK_INF);
+    }
+    if (!grid_barrier(a)) break;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
+  if (lane == 0 && evals) atomicAdd(a.node_evals, evals);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *a.rs.rounds = r;
+    if (r >= a.rs.max_rounds) {
+      atomicOr(a.err, ERRB_NOT_CONVERGED);
+      atomicExch(a.abort_flag, 1);
     }
   }
 }
@@ -534,7 +487,7 @@ void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs
                         const ForwardBatch& fb, const SolveArgs& sa, cudaStream_t st) {
   const long long N = npts(hprobs[0].g);
   coarse_init_kernel<<<1184, 256, 0, st>>>(dprobs, nprob, N);
-  queue_init_kernel<<<296, 256, 0, st>>>(sa);
+  rounds_init_kernel<<<296, 256, 0, st>>>(sa);
   if (sa.nd == 3) seed_kernel<3><<<nprob, 128, 0, st>>>(sa, fb);
   else seed_kernel<2><<<nprob, 128, 0, st>>>(sa, fb);
 }
@@ -542,22 +495,19 @@ void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs
 void launch_queue_init(const SolveArgs& sa, cudaStream_t st) { queue_init_kernel<<<296, 256, 0, st>>>(sa); }
 
 template <int ND>
-static void launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st) {
-  const size_t sm = sizeof(TileSmem<ND>) * SOLVE_WARPS;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(coarse_solve_kernel<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    attr = true;
-  }
+static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st) {
   int per = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_solve_kernel<ND>, SOLVE_THREADS, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND>, SOLVE_THREADS, 0);
   per = per < 1 ? 1 : per;
-  coarse_solve_kernel<ND><<<nsm * per, SOLVE_THREADS, sm, st>>>(sa);
+  SolveArgs args = sa;
+  void* kargs[] = {&args};
+  // cooperative: every CTA is resident, so the grid barrier between rounds cannot deadlock
+  return cudaLaunchCooperativeKernel((const void*)coarse_rounds_kernel<ND>, dim3(nsm * per), dim3(SOLVE_THREADS),
+                                     kargs, 0, st);
 }
 
-void launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st) {
-  if (sa.nd == 3) launch_solve_nd<3>(sa, nsm, st);
-  else launch_solve_nd<2>(sa, nsm, st);
+cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st) {
+  return sa.nd == 3 ? launch_solve_nd<3>(sa, nsm, st) : launch_solve_nd<2>(sa, nsm, st);
 }
 
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,

@@ -64,6 +64,7 @@ struct CoarseProblem {
   int32_t pad;
   long long tbase; // first global tile id of this problem
   double tinv;     // QBUCKETS / (time scale of this problem): trigger time -> bucket
+  double delta;    // round width of the forward solve (traveltime units)
 };
 
 // Bucketed priority queue of tile ids: QBUCKETS bounded multi-producer/multi-consumer
@@ -77,6 +78,21 @@ struct TileQueue {
   unsigned long long* head;   // QBUCKETS
   unsigned long long* tail;   // QBUCKETS
   unsigned long long mask;
+};
+
+// Worklists and thresholds of the round-synchronous forward solve. Nodes are numbered
+// globally over the problems of a call: problem * N + node.
+struct RoundState {
+  int32_t* stamp;               // per node: last round it was listed for
+  double* tent;                 // per node: value of its last evaluation
+  uint8_t* dirty;               // per node: something it reads changed since that evaluation
+  unsigned int* list[2];        // node ids of the current and the next round
+  unsigned int* cnt;            // [3] list length per round (mod 3)
+  unsigned int* grab;           // [3] next list entry to take per round (mod 3)
+  unsigned long long* nextmin;  // [3][nprob] smallest pending potential (double bits)
+  unsigned int* bar;            // [2] grid barrier: arrivals, generation
+  int32_t* rounds;              // rounds run
+  int32_t max_rounds;
 };
 
 struct SolveArgs {
@@ -97,6 +113,7 @@ struct SolveArgs {
   int32_t max_passes;
   double gate;                 // in-tile front gate, in units of (node spacing x slowness)
   long long timeout_ns;
+  RoundState rs;
 };
 
 constexpr uint32_t FACES_ALL = 1u << 6;
@@ -107,7 +124,7 @@ void launch_fine(const ForwardBatch& fb, cudaStream_t st);
 size_t fine_smem_bytes(int heapcap);
 void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs, int nprob,
                         const ForwardBatch& fb, const SolveArgs& sa, cudaStream_t st);
-void launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
+cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
 void launch_queue_init(const SolveArgs& sa, cudaStream_t st);  // empty queue, idle tiles, zero counters
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);

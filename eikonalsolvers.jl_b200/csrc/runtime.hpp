@@ -39,6 +39,7 @@ struct Model {
   double* vel = nullptr;   // device
   double* slow = nullptr;  // device, 1.0/vel
   double tscale = 1.0;     // grid diagonal x mean slowness (tile scheduling only)
+  double smin = 0.0;       // smallest slowness of the model (round width of the forward solve)
 };
 
 // Device results of the forward stage of one call.
@@ -72,6 +73,7 @@ struct eik_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // whole call
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
+  double round_gate = 1.0;  // forward round width in units of (smallest spacing x smallest slowness)
   std::mutex mu;
   eik::Scratch scratch;
   size_t model_bytes = 0;

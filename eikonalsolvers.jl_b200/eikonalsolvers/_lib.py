@@ -21,7 +21,8 @@ ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EI
 
 EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last_error",
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
-            "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc"]
+            "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc",
+            "eik_ctx_set_param"]
 
 
 class EikError(RuntimeError):
@@ -50,7 +51,7 @@ class eik_stats(C.Structure):
     _fields_ = [("warn_mask", C.c_uint32), ("err_mask", C.c_uint32), ("tile_activations", C.c_uint64),
                 ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
                 ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_activations", C.c_uint64),
-                ("launches", C.c_uint64)]
+                ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64)]
 
 
 _lib = None
@@ -84,6 +85,8 @@ def load():
                                           C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
         L.eik_ttimemisfit_noalloc.argtypes = [C.POINTER(eik_grid), C.c_int64, P, P, P, P, P, P, P]
         L.eik_ttimemisfit_noalloc.restype = C.c_int
+        L.eik_ctx_set_param.argtypes = [P, C.c_char_p, C.c_double]
+        L.eik_ctx_set_param.restype = C.c_int
         L.eik_ctx_stream.argtypes = [P]
         L.eik_ctx_stream.restype = C.c_void_p
         for f in ("eik_ctx_create", "eik_ctx_destroy", "eik_model_upload", "eik_model_upload_device",

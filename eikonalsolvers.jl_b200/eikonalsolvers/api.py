@@ -34,6 +34,10 @@ class Context:
         self.device = device
         self.last_stats = _lib.eik_stats()
 
+    def set_param(self, name: str, value: float):
+        """Scheduling parameter of this context (see eik_ctx_set_param)."""
+        _lib.check(self.L.eik_ctx_set_param(self.h, name.encode(), float(value)), self.h)
+
     def close(self):
         if self.h:
             self.L.eik_ctx_destroy(self.h)

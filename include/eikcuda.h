@@ -93,7 +93,7 @@ typedef struct {
 typedef struct {
   uint32_t warn_mask;        /* EIK_WARN_* */
   uint32_t err_mask;         /* device error word of the last launch (0 = none) */
-  uint64_t tile_activations; /* coarse tiles processed */
+  uint64_t tile_activations; /* forward solve: listed nodes visited over all rounds */
   uint64_t node_evals;       /* coarse node updates evaluated */
   double device_ms;          /* device time of the call (CUDA events) */
   double fine_ms;            /* start-up stage: refined-grid FMM or source box (CUDA events) */
@@ -101,6 +101,7 @@ typedef struct {
   double adj_ms;             /* adjoint dataflow solve kernel (CUDA events) */
   uint64_t adj_activations;  /* adjoint tiles processed */
   uint64_t launches;         /* kernels this call launched */
+  uint64_t fwd_rounds;       /* rounds of the forward solve */
 } eik_stats;
 
 /* Fills the reference defaults of ExtraParams(). */
@@ -114,6 +115,11 @@ const char* eik_last_error(eik_ctx* ctx);
 /* The CUDA stream (cudaStream_t) all work of this context runs on, for callers that order
  * their own work or events against it. */
 void* eik_ctx_stream(eik_ctx* ctx);
+/* Scheduling parameters of a context (results do not depend on them, only the amount of
+ * work does): "round_gate" = width of a forward round in units of (smallest node spacing x
+ * smallest slowness), default 1. Returns EIK_ERR_ASSERT for an unknown name or a value
+ * out of range. */
+int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 
 /* Uploads a velocity model (host, column-major, FP64) and keeps it resident. Checks
  * all(vel.>0) (eikmainfwd.jl:45). */
