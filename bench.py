@@ -410,7 +410,7 @@ def main_b200(args):
             "clocks": clocks,
             "gpu_launches": int(launches),
             "stats": {"tile_activations": int(st.tile_activations), "node_evals": int(st.node_evals),
-                      "adj_activations": int(st.adj_activations), "evals_per_node": st.node_evals / (N * nsrc)},
+                      "adj_rounds": int(st.adj_rounds), "fwd_rounds": int(st.fwd_rounds), "evals_per_node": st.node_evals / (N * nsrc)},
         }
         print(json.dumps(line), flush=True)
     ctx.release(mid)

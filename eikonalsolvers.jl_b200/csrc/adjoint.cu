@@ -15,6 +15,7 @@
 
 #include "../../include/eikcuda.h"
 #include "queue.cuh"
+#include "rounds.cuh"
 #include "runtime.hpp"
 
 namespace eik {
@@ -51,7 +52,10 @@ __device__ __forceinline__ bool is_source(const CoarseProblem& P, long long l) {
 }
 
 // ------------------------------------------------------------ per-node preparation --
-__global__ void adj_prep_kernel(const CoarseProblem* probs, const AdjProblem* ap, int nprob, long long N) {
+// Also counts, for every node, the nodes whose stencil reads it (its dependants in Jᵀλ = b)
+// and lists the nodes without any for round 0 of the solve.
+__global__ void adj_prep_kernel(const CoarseProblem* probs, const AdjProblem* ap, int nprob, long long N,
+                                SolveArgs sa) {
   const long long tot = N * nprob;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
     const int s = (int)(q / N);
@@ -81,6 +85,26 @@ __global__ void adj_prep_kernel(const CoarseProblem* probs, const AdjProblem* ap
         v = 2.0 * tmp1;
       }
       A.gdt[(long long)a * N + l] = v;
+    }
+    int ndep = 0;
+    for (int ax = 0; ax < g.nd; ax++)
+      for (int dl = -2; dl <= 2; dl++) {
+        if (dl == 0) continue;
+        int pr[3] = {i, j, k};
+        pr[ax] += dl;
+        if (pr[ax] < 0 || pr[ax] >= g.n[ax]) continue;
+        int8_t cr[3];
+        unpack_codes(P.code[lin3(g, pr[0], pr[1], pr[2])], cr);
+        const int cc = cr[ax];
+        if (cc == 0) continue;
+        const int ac = cc < 0 ? -cc : cc;
+        const int p = -dl * (cc > 0 ? -1 : 1);
+        if (p >= 1 && p <= ac) ndep++;
+      }
+    sa.rs.stamp[q] = ndep;
+    if (ndep == 0 && !src) {
+      const unsigned int at = atomicAdd(sa.rs.cnt, 1u);
+      sa.rs.list[0][at] = (unsigned int)q;
     }
   }
 }
@@ -221,273 +245,128 @@ __global__ void adj_recv_kernel(RecvArgs ra) {
   ra.misfit[s] = misf;
 }
 
-// ----------------------------------------------------------- dataflow adjoint solve --
-template <int ND>
-struct AdjSmem {
-  using C = TileCfg<ND>;
-  static constexpr int TN = C::TX * C::TY * C::TZ;
-  static constexpr int HN = C::HX * C::HY * C::HZ;
-  double lam[HN];
-  double gdt[ND][HN];
-  uint8_t code[HN];
-  uint8_t fin[HN];
-  uint8_t newfin[TN];
-};
-constexpr int ADJ_THREADS = 128;
-constexpr int ADJ_WARPS = ADJ_THREADS / 32;
-
-template <int ND>
-__device__ __forceinline__ int ahidx(int x, int y, int z) {
-  using C = TileCfg<ND>;
-  return (x + C::H) + C::HX * ((y + C::H) + C::HY * (ND == 3 ? z + C::H : 0));
+// ------------------------------------------------------------- adjoint solve --
+// Jᵀλ = b in topological order of the stencil graph (Kahn): round r takes the nodes whose
+// dependants are all final, computes
+//   λ_i = (b_i − Σ_{r reads i} J[r,i] λ_r) / J[i,i]
+// pulling the dependants' λ in a fixed order (deterministic), then releases the nodes its
+// own stencil reads; a node whose dependant count drops to zero is listed for the next
+// round. Every node is computed exactly once, after everything it depends on.
+__global__ void adj_rounds_init_kernel(SolveArgs a) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int k = 0; k < 3; k++) {
+    a.rs.cnt[k] = 0;
+    a.rs.grab[k] = 0;
+  }
+  a.rs.bar[0] = 0;
+  a.rs.bar[1] = 0;
+  *a.rs.rounds = 0;
+  *a.abort_flag = 0;
 }
 
 template <int ND>
-__device__ int adj_process_tile(const AdjArgs& aa, AdjSmem<ND>& S, int prob, long long tile, double* prio_out) {
-  using C = TileCfg<ND>;
-  constexpr int TN = AdjSmem<ND>::TN, HN = AdjSmem<ND>::HN;
-  constexpr int NPT = (TN + 31) / 32;
+__device__ void adj_node(const AdjArgs& aa, int prob, long long l, unsigned long long gb, unsigned int* rel) {
   const SolveArgs& a = aa.sa;
   const CoarseProblem& P = a.probs[prob];
   const AdjProblem& A = aa.ap[prob];
   const GridDesc& g = P.g;
   const long long N = npts(g);
-  const int tx = (int)(tile % P.nt[0]);
-  const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
-  const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
-  const int ox = tx * C::TX, oy = ty * C::TY, oz = tz * C::TZ;
-  const int lane = threadIdx.x & 31;
-  for (int h = lane; h < HN; h += 32) {
-    const int hx = h % C::HX, hy = (h / C::HX) % C::HY, hz = h / (C::HX * C::HY);
-    const int gx = ox + hx - C::H, gy = oy + hy - C::H, gz = (ND == 3) ? oz + hz - C::H : 0;
-    if (gx >= 0 && gx < g.n[0] && gy >= 0 && gy < g.n[1] && gz >= 0 && gz < g.n[2]) {
-      const long long l = lin3(g, gx, gy, gz);
-      // λ and the final flags change under other SMs: L2-coherent loads
-      const double v = __ldcg(A.lam + l);
-      S.lam[h] = v;
-      S.fin[h] = !lam_pending(v);
-      S.code[h] = __ldg(P.code + l);
+  const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
+  const uint8_t cb = P.code[l];
+  int8_t cm[3];
+  unpack_codes(cb, cm);
+  if ((cb & CODE_SRC_BIT) && P.kL[l] == -EIK_INF) return;  // source points: no unknown
+  double sum = A.rhs[l];
+  double dh[3];
 #pragma unroll
-      for (int d = 0; d < ND; d++) S.gdt[d][h] = __ldg(A.gdt + (long long)d * N + l);
-    } else {
-      S.lam[h] = 0.0;
-      S.code[h] = CODE_NONE;
-      S.fin[h] = 1;
+  for (int ax = 0; ax < ND; ax++)
 #pragma unroll
-      for (int d = 0; d < ND; d++) S.gdt[d][h] = 0.0;
+    for (int dl = -2; dl <= 2; dl++) {
+      if (dl == 0) continue;
+      int pr[3] = {c[0], c[1], c[2]};
+      pr[ax] += dl;
+      if (pr[ax] < 0 || pr[ax] >= g.n[ax]) continue;
+      const long long lr = lin3(g, pr[0], pr[1], pr[2]);
+      int8_t cd[3];
+      unpack_codes(P.code[lr], cd);
+      const int cc = cd[ax];
+      if (cc == 0) continue;
+      const int ac = cc < 0 ? -cc : cc;
+      const int sg = cc > 0 ? -1 : 1;
+      const int p = -dl * sg;
+      if (p < 1 || p > ac) continue;
+      node_dh(g, pr[0], dh);
+      const double J = A.gdt[(long long)ax * N + lr] * ((double)sg * dcoeff(ac, p, dh[ax]));
+      sum -= J * __ldcg(A.lam + lr);
+    }
+  node_dh(g, c[0], dh);
+  double dg = 0.0;
+  bool first = true;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++) {
+    if (cm[ax] == 0) continue;
+    const int ac = cm[ax] < 0 ? -cm[ax] : cm[ax];
+    const int sg = cm[ax] > 0 ? -1 : 1;
+    const double v = A.gdt[(long long)ax * N + l] * ((double)sg * dcoeff(ac, 0, dh[ax]));
+    dg = first ? v : dg + v;
+    first = false;
+  }
+  A.lam[l] = sum / dg;
+  __threadfence();
+  // release the nodes this node's stencil reads
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++) {
+    const int ac = cm[ax] < 0 ? -cm[ax] : cm[ax];
+    const int sg = cm[ax] > 0 ? -1 : 1;
+    for (int p = 1; p <= ac; p++) {
+      int q[3] = {c[0], c[1], c[2]};
+      q[ax] += sg * p;
+      const long long lu = lin3(g, q[0], q[1], q[2]);
+      if (atomicSub(a.rs.stamp + gb + lu, 1) == 1) rel[2 * ax + p - 1] = (unsigned int)(gb + lu);
     }
   }
-  for (int li = lane; li < TN; li += 32) S.newfin[li] = 0;
-  __syncwarp();
-  int fm = 0;
-  double tmin = EIK_INF;
-  for (int pass = 0; pass < 4 * TN; pass++) {
-    double nl[NPT];
-    int nli[NPT];
-    bool progress = false;
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      nli[r] = -1;
-      const int li = lane + 32 * r;
-      if (li >= TN) continue;
-      const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-      const int c[3] = {ox + x, oy + y, oz + z};
-      if (c[0] >= g.n[0] || c[1] >= g.n[1] || c[2] >= g.n[2]) continue;
-      const int hm = ahidx<ND>(x, y, z);
-      if (S.fin[hm]) continue;
-      const long long l = lin3(g, c[0], c[1], c[2]);
-      double sum = A.rhs[l];
-      bool ready = true;
-      double dh[3];
-      for (int ax = 0; ax < ND && ready; ax++)
-        for (int dl = -2; dl <= 2 && ready; dl++) {
-          if (dl == 0) continue;
-          int pr[3] = {c[0], c[1], c[2]};
-          pr[ax] += dl;
-          if (pr[ax] < 0 || pr[ax] >= g.n[ax]) continue;
-          int q[3] = {x, y, z};
-          q[ax] += dl;
-          const int hr = ahidx<ND>(q[0], q[1], q[2]);
-          int8_t cd[3];
-          unpack_codes(S.code[hr], cd);
-          const int cc = cd[ax];
-          if (cc == 0) continue;
-          const int ac = cc < 0 ? -cc : cc;
-          const int sg = cc > 0 ? -1 : 1;
-          const int p = -dl * sg;
-          if (p < 1 || p > ac) continue;
-          if (!S.fin[hr]) {
-            ready = false;
-            break;
-          }
-          node_dh(g, pr[0], dh);
-          const double J = S.gdt[ax][hr] * ((double)sg * dcoeff(ac, p, dh[ax]));
-          sum -= J * S.lam[hr];
-        }
-      if (!ready) continue;
-      // diagonal
-      int8_t cm[3];
-      unpack_codes(S.code[hm], cm);
-      node_dh(g, c[0], dh);
-      double dg = 0.0;
-      bool first = true;
-      for (int ax = 0; ax < ND; ax++) {
-        if (cm[ax] == 0) continue;
-        const int ac = cm[ax] < 0 ? -cm[ax] : cm[ax];
-        const int sg = cm[ax] > 0 ? -1 : 1;
-        const double v = S.gdt[ax][hm] * ((double)sg * dcoeff(ac, 0, dh[ax]));
-        dg = first ? v : dg + v;
-        first = false;
-      }
-      nl[r] = sum / dg;
-      nli[r] = li;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int r = 0; r < NPT; r++) {
-      const int li = nli[r];
-      if (li < 0) continue;
-      const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-      const int hm = ahidx<ND>(x, y, z);
-      S.lam[hm] = nl[r];
-      S.fin[hm] = 1;
-      S.newfin[li] = 1;
-      progress = true;
-      int f = 0;
-      if (x < 2) f |= 1;
-      if (x >= C::TX - 2) f |= 2;
-      if (y < 2) f |= 4;
-      if (y >= C::TY - 2) f |= 8;
-      if (ND == 3 && z < 2) f |= 16;
-      if (ND == 3 && z >= C::TZ - 2) f |= 32;
-      if (f) {
-        fm |= f;
-        tmin = fmin(tmin, P.t[lin3(g, ox + x, oy + y, oz + z)]);
-      }
-    }
-    __syncwarp();
-    if (!__any_sync(0xffffffffu, progress)) break;
-  }
-  for (int li = lane; li < TN; li += 32) {
-    if (!S.newfin[li]) continue;
-    const int x = li % C::TX, y = (li / C::TX) % C::TY, z = li / (C::TX * C::TY);
-    const long long l = lin3(g, ox + x, oy + y, oz + z);
-    const int hm = ahidx<ND>(x, y, z);
-    A.lam[l] = S.lam[hm];  // one 64-bit store publishes value and state together
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    fm |= __shfl_xor_sync(0xffffffffu, fm, o);
-    tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
-  }
-  // reverse-time priority: later traveltimes first
-  *prio_out = fmax(0.0, (double)QBUCKETS / P.tinv - tmin);
-  return fm;
 }
 
 template <int ND>
-__global__ void __launch_bounds__(ADJ_THREADS) adj_solve_kernel(AdjArgs aa) {
-  extern __shared__ __align__(16) unsigned char adj_smem[];
+__global__ void __launch_bounds__(SOLVE_THREADS) adj_rounds_kernel(AdjArgs aa) {
   const SolveArgs& a = aa.sa;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  AdjSmem<ND>& S = reinterpret_cast<AdjSmem<ND>*>(adj_smem)[warp];
-  long long idle_since = -1;
-  for (;;) {
-    int ab = (lane == 0) ? *(volatile int*)a.abort_flag : 0;
-    if (__shfl_sync(0xffffffffu, ab, 0)) break;
-    unsigned long long its[QCLAIM] = {0, 0, 0, 0};
-    const int ngot = q_pop_warp(a, its);
-    if (!ngot) {
-      int done = (lane == 0) ? (*(volatile int*)a.pending == 0) : 0;
-      if (__shfl_sync(0xffffffffu, done, 0)) break;
-      if (lane == 0) {
-        const long long now = gtimer_ns();
-        if (idle_since < 0) idle_since = now;
-        if (now - idle_since > a.timeout_ns) {
-          atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
-          atomicExch(a.abort_flag, 1);
-        }
-        __nanosleep(200);
+  const int lane = threadIdx.x & 31;
+  const unsigned long long N = (unsigned long long)npts(a.probs[0].g);
+  int r = 0;
+  for (; r < a.rs.max_rounds; r++) {
+    const int b3 = r % 3;
+    const unsigned int n = *(volatile unsigned int*)(a.rs.cnt + b3);
+    if (n == 0) break;
+    const unsigned int* L = a.rs.list[r & 1];
+    for (;;) {
+      unsigned int base = 0;
+      if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base >= n) break;
+      const unsigned int idx = base + lane;
+      unsigned int rel[6] = {~0u, ~0u, ~0u, ~0u, ~0u, ~0u};
+      if (idx < n) {
+        const unsigned int gid = L[idx];
+        const int prob = (int)(gid / N);
+        const unsigned long long gb = (unsigned long long)prob * N;
+        adj_node<ND>(aa, prob, (long long)(gid - gb), gb, rel);
       }
-      __syncwarp();
-      continue;
+#pragma unroll
+      for (int k = 0; k < 2 * ND; k++) warp_append(a, r + 1, rel[k] != ~0u, rel[k]);
     }
-    idle_since = -1;
-    for (int j = 0; j < ngot; j++) {
-      const unsigned long long it = its[j];
-      const int prob = (int)(it >> 40);
-      const long long tile = (long long)(it & ((1ull << 40) - 1));
-      const long long gt = a.probs[prob].tbase + tile;
-      if (lane == 0) {
-        atomicExch(a.tile_flag + gt, TS_BUSY);
-        atomicExch(a.tile_faces + gt, 0u);
-        atomicExch(a.tile_prio + gt, (unsigned long long)__double_as_longlong(EIK_INF));
-        __threadfence();
-        const unsigned long long na = atomicAdd(a.activations, 1ull);
-        if (na > a.max_activations) {
-          atomicOr(a.err, ERRB_ADJ_NOT_CONVERGED);
-          atomicExch(a.abort_flag, 1);
-        }
-      }
-      __syncwarp();
-      double pr;
-      const int fm = adj_process_tile<ND>(aa, S, prob, tile, &pr);
-      __threadfence();
-      __syncwarp();
-      if (lane == 0) {
-        const CoarseProblem& P = a.probs[prob];
-        const int tx = (int)(tile % P.nt[0]);
-        const int ty = (int)((tile / P.nt[0]) % P.nt[1]);
-        const int tz = (int)(tile / ((long long)P.nt[0] * P.nt[1]));
-        auto nbt = [&](int x, int y, int z) { return (long long)x + (long long)P.nt[0] * (y + (long long)P.nt[1] * z); };
-        if ((fm & 1) && tx > 0) enqueue_tile(a, prob, nbt(tx - 1, ty, tz), 2u, pr);
-        if ((fm & 2) && tx + 1 < P.nt[0]) enqueue_tile(a, prob, nbt(tx + 1, ty, tz), 1u, pr);
-        if ((fm & 4) && ty > 0) enqueue_tile(a, prob, nbt(tx, ty - 1, tz), 8u, pr);
-        if ((fm & 8) && ty + 1 < P.nt[1]) enqueue_tile(a, prob, nbt(tx, ty + 1, tz), 4u, pr);
-        if (ND == 3) {
-          if ((fm & 16) && tz > 0) enqueue_tile(a, prob, nbt(tx, ty, tz - 1), 32u, pr);
-          if ((fm & 32) && tz + 1 < P.nt[2]) enqueue_tile(a, prob, nbt(tx, ty, tz + 1), 16u, pr);
-        }
-        __threadfence();
-        finish_tile(a, prob, tile);
-      }
-      __syncwarp();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const int c3 = (r + 2) % 3;
+      a.rs.cnt[c3] = 0;
+      a.rs.grab[c3] = 0;
     }
+    if (!grid_barrier(a)) break;
   }
-}
-
-// The dataflow starts from the nodes no stencil depends on (the late ends of the
-// characteristics: local maxima of t); their tiles are queued, latest times first.
-template <int ND>
-__global__ void adj_roots_kernel(SolveArgs a, long long N) {
-  using Cfg = TileCfg<ND>;
-  const long long tot = N * a.nprob;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-    const int s = (int)(q / N);
-    const long long l = q - (long long)s * N;
-    const CoarseProblem& P = a.probs[s];
-    const GridDesc& g = P.g;
-    if (is_source(P, l)) continue;
-    const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
-    bool root = true;
-    for (int ax = 0; ax < ND && root; ax++)
-      for (int dl = -2; dl <= 2 && root; dl++) {
-        if (dl == 0) continue;
-        int pr[3] = {c[0], c[1], c[2]};
-        pr[ax] += dl;
-        if (pr[ax] < 0 || pr[ax] >= g.n[ax]) continue;
-        int8_t cd[3];
-        unpack_codes(P.code[lin3(g, pr[0], pr[1], pr[2])], cd);
-        const int cc = cd[ax];
-        if (cc == 0) continue;
-        const int ac = cc < 0 ? -cc : cc;
-        const int p = -dl * (cc > 0 ? -1 : 1);
-        if (p >= 1 && p <= ac) root = false;
-      }
-    if (!root) continue;
-    const long long tile = (long long)(c[0] / Cfg::TX) +
-                           (long long)P.nt[0] * ((long long)(c[1] / Cfg::TY) + (long long)P.nt[1] * (c[2] / Cfg::TZ));
-    enqueue_tile(a, s, tile, FACES_ALL, fmax(0.0, (double)QBUCKETS / P.tinv - P.t[l]));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *a.rs.rounds = r;
+    if (r >= a.rs.max_rounds) {
+      atomicOr(a.err, ERRB_ADJ_NOT_CONVERGED);
+      atomicExch(a.abort_flag, 1);
+    }
   }
 }
 
@@ -1022,17 +901,15 @@ __global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int nw, long long
 }
 
 template <int ND>
-static void launch_adj_solve(const AdjArgs& aa, int nsm, cudaStream_t st) {
-  const size_t sm = sizeof(AdjSmem<ND>) * ADJ_WARPS;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(adj_solve_kernel<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    attr = true;
-  }
+static cudaError_t launch_adj_solve(const AdjArgs& aa, int nsm, cudaStream_t st) {
   int per = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, adj_solve_kernel<ND>, ADJ_THREADS, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, adj_rounds_kernel<ND>, SOLVE_THREADS, 0);
   per = per < 1 ? 1 : per;
-  adj_solve_kernel<ND><<<nsm * per, ADJ_THREADS, sm, st>>>(aa);
+  AdjArgs args = aa;
+  void* kargs[] = {&args};
+  // cooperative: every CTA is resident, so the grid barrier between rounds cannot deadlock
+  return cudaLaunchCooperativeKernel((const void*)adj_rounds_kernel<ND>, dim3(nsm * per), dim3(SOLVE_THREADS),
+                                     kargs, 0, st);
 }
 
 }  // namespace eik
@@ -1131,7 +1008,14 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   CUDA_OK(ctx, cudaMemsetAsync(dwarn, 0, sizeof(uint32_t), st));
   CUDA_OK(ctx, cudaMemsetAsync(gsrc, 0, sizeof(double) * nsrc * nd, st));
   const CoarseProblem* dprobs = fw.sa.probs;
-  adj_prep_kernel<<<2 * ctx->nsm * 8, 256, 0, st>>>(dprobs, dap, (int)nsrc, N);
+  // the adjoint sweep reuses the forward's worklists; counts live in its round stamps
+  AdjArgs aa;
+  aa.sa = fw.sa;
+  aa.ap = dap;
+  aa.sa.rs.max_rounds = 1 << 26;
+  aa.sa.rs.rounds = fw.sa.rs.rounds + 1;  // the forward's count stays readable
+  adj_rounds_init_kernel<<<1, 1, 0, st>>>(aa.sa);
+  adj_prep_kernel<<<2 * ctx->nsm * 8, 256, 0, st>>>(dprobs, dap, (int)nsrc, N, aa.sa);
   RecvArgs ra;
   ra.g = m.g;
   ra.nsrc = (int)nsrc;
@@ -1145,19 +1029,8 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   ra.misfit = misf;
   ra.dpsi = dpsi;
   adj_recv_kernel<<<(int)((nsrc + 63) / 64), 64, 0, st>>>(ra);
-  // dataflow solve, reusing the forward's tile state arrays and queue
-  AdjArgs aa;
-  aa.sa = fw.sa;
-  aa.ap = dap;
-  aa.sa.max_activations = 400ull * (unsigned long long)fw.sa.ntiles + 100000ull;
-  aa.sa.activations = fw.sa.activations + 4;  // own counters; the forward's stay readable
-  aa.sa.node_evals = fw.sa.activations + 5;
-  launch_queue_init(aa.sa, st);
-  if (nd == 3) adj_roots_kernel<3><<<ctx->nsm * 8, 256, 0, st>>>(aa.sa, N);
-  else adj_roots_kernel<2><<<ctx->nsm * 8, 256, 0, st>>>(aa.sa, N);
   cudaEventRecord(ctx->evk[4], st);
-  if (nd == 3) launch_adj_solve<3>(aa, ctx->nsm, st);
-  else launch_adj_solve<2>(aa, ctx->nsm, st);
+  CUDA_OK(ctx, nd == 3 ? launch_adj_solve<3>(aa, ctx->nsm, st) : launch_adj_solve<2>(aa, ctx->nsm, st));
   cudaEventRecord(ctx->evk[5], st);
   adj_check_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, N, fw.fb.err);
   CUDA_OK(ctx, cudaGetLastError());
@@ -1193,14 +1066,14 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
     CUDA_OK(ctx, cudaMemcpyAsync(d_gradsrc, gsrc, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToDevice, st));
   CUDA_OK(ctx, cudaGetLastError());
   uint32_t hw = 0;
-  unsigned long long actr[2] = {0, 0};
+  int32_t arounds = 0;
   CUDA_OK(ctx, cudaMemcpyAsync(&hw, dwarn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  CUDA_OK(ctx, cudaMemcpyAsync(actr, aa.sa.activations, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(&arounds, aa.sa.rs.rounds, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   rc = collect_forward_stats(ctx, &fw, stats);
   if (stats) {
     stats->warn_mask |= hw;
-    stats->adj_activations = actr[0];
-    stats->launches += 8 + (d_misfit ? 1 : 0) +
+    stats->adj_rounds = (uint64_t)arounds;
+    stats->launches += 7 + (d_misfit ? 1 : 0) +
                        (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->evk[4], ctx->evk[5]);

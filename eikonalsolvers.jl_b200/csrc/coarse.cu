@@ -13,6 +13,7 @@
 // is bounded; both report through an error word instead of trapping.
 #include "kernels.cuh"
 #include "queue.cuh"
+#include "rounds.cuh"
 
 namespace eik {
 
@@ -149,45 +150,6 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long* p, double v) 
   // traveltimes and potentials are >= 0: their bit patterns order as the values
   if (v < EIK_INF && v < __longlong_as_double((long long)ld_volatile(p)))
     atomicMin(p, (unsigned long long)__double_as_longlong(v));
-}
-
-// Grid-wide barrier of the cooperative solve launch (all CTAs co-resident). The wait is
-// bounded by the global timer; a CTA that gives up raises the abort flag, which releases
-// the others. Returns false when the solve is aborted.
-__device__ bool grid_barrier(const SolveArgs& a) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    volatile unsigned int* gen = a.rs.bar + 1;
-    const unsigned int g0 = *gen;
-    const unsigned int arrived = atomicAdd(a.rs.bar, 1u);
-    bool ok = true;
-    if (arrived == gridDim.x - 1) {
-      atomicExch(a.rs.bar, 0u);
-      __threadfence();
-      atomicAdd(a.rs.bar + 1, 1u);
-    } else {
-      const long long t0 = gtimer_ns();
-      while (*gen == g0) {
-        if (*(volatile int*)a.abort_flag) {
-          ok = false;
-          break;
-        }
-        if (gtimer_ns() - t0 > a.timeout_ns) {
-          atomicOr(a.err, ERRB_QUEUE_TIMEOUT);
-          atomicExch(a.abort_flag, 1);
-          ok = false;
-          break;
-        }
-        __nanosleep(40);
-      }
-    }
-    __threadfence();
-    s_ok = ok && !*(volatile int*)a.abort_flag;
-  }
-  __syncthreads();
-  return s_ok != 0;
 }
 
 // One listed node: gate, evaluate, write back. Returns the directions of the nodes to list

@@ -50,7 +50,7 @@ class eik_extra(C.Structure):
 class eik_stats(C.Structure):
     _fields_ = [("warn_mask", C.c_uint32), ("err_mask", C.c_uint32), ("tile_activations", C.c_uint64),
                 ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
-                ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_activations", C.c_uint64),
+                ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_rounds", C.c_uint64),
                 ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64)]
 
 

@@ -99,7 +99,7 @@ typedef struct {
   double fine_ms;            /* start-up stage: refined-grid FMM or source box (CUDA events) */
   double solve_ms;           /* coarse forward solve kernel (CUDA events) */
   double adj_ms;             /* adjoint dataflow solve kernel (CUDA events) */
-  uint64_t adj_activations;  /* adjoint tiles processed */
+  uint64_t adj_rounds;       /* rounds of the adjoint sweep */
   uint64_t launches;         /* kernels this call launched */
   uint64_t fwd_rounds;       /* rounds of the forward solve */
 } eik_stats;
