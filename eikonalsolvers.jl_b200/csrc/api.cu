@@ -302,6 +302,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
       double hmin = dh[0];
       for (int a = 1; a < g.nd; a++) hmin = std::min(hmin, dh[a]);
       P.delta = ctx->round_gate * hmin * m.smin;
+      P.incmin = 0.999 * (2.0 / 3.0) * hmin * m.smin / std::sqrt((double)g.nd);
     }
   }
   CoarseProblem* dp;
@@ -337,13 +338,15 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   GET(sa.rs.list[0], unsigned int, "rs_list0", nsrc * N);
   GET(sa.rs.list[1], unsigned int, "rs_list1", nsrc * N);
   GET(sa.rs.nextmin, unsigned long long, "rs_nextmin", 3 * nsrc);
+  GET(sa.rs.thr, double, "rs_thr", 2 * nsrc);
   {
     unsigned int* rc32;
-    GET(rc32, unsigned int, "rs_ctr", 16);
+    GET(rc32, unsigned int, "rs_ctr", 32);
     sa.rs.cnt = rc32;
     sa.rs.grab = rc32 + 3;
     sa.rs.bar = rc32 + 6;
     sa.rs.rounds = (int32_t*)(rc32 + 8);
+    sa.rs.visits = reinterpret_cast<unsigned long long*>(rc32 + 12);  // 8-byte aligned: 7 counters
   }
   sa.rs.max_rounds = 1 << 24;
   sa.err = fb.err;
@@ -383,7 +386,9 @@ int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
   unsigned long long ctr[4] = {0, 0, 0, 0};
   uint32_t e = 0;
   int32_t rounds = 0;
+  unsigned long long vis[7] = {0, 0, 0, 0, 0, 0, 0};
   cudaMemcpyAsync(ctr + 2, fw->sa.activations, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(vis, fw->sa.rs.visits, sizeof vis, cudaMemcpyDeviceToHost, ctx->stream);
   cudaMemcpyAsync(&rounds, fw->sa.rs.rounds, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
   cudaMemcpyAsync(&e, fw->fb.err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream);
   std::vector<SrcOut> outs(fw->nsrc);
@@ -397,6 +402,7 @@ int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
     stats->tile_activations += ctr[2];
     stats->node_evals += ctr[3];
     stats->fwd_rounds += (uint64_t)rounds;
+    for (int k = 0; k < 7; k++) stats->fwd_visits[k] += vis[k];
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, ctx->evk[0], ctx->evk[1]);
     cudaEventElapsedTime(&b, ctx->evk[2], ctx->evk[3]);

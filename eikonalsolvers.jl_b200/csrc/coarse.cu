@@ -72,6 +72,9 @@ __global__ void rounds_init_kernel(SolveArgs a) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < 3LL * a.nprob;
        q += (long long)gridDim.x * blockDim.x)
     a.rs.nextmin[q] = (unsigned long long)__double_as_longlong(EIK_INF);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < 2LL * a.nprob;
+       q += (long long)gridDim.x * blockDim.x)
+    a.rs.thr[q] = -EIK_INF;
   if (blockIdx.x == 0 && threadIdx.x < 3) {
     a.rs.cnt[threadIdx.x] = 0;
     a.rs.grab[threadIdx.x] = 0;
@@ -80,6 +83,7 @@ __global__ void rounds_init_kernel(SolveArgs a) {
     a.rs.bar[0] = 0;
     a.rs.bar[1] = 0;
     *a.rs.rounds = 0;
+    for (int k = 0; k < 7; k++) a.rs.visits[k] = 0;
     *a.pending = 0;
     *a.activations = 0;
     *a.node_evals = 0;
@@ -157,7 +161,8 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long* p, double v) 
 // bounds their next evaluation from below.
 template <int ND>
 __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, unsigned long long gbase, long long l,
-                                 double T, int r, double* front, unsigned long long* evals) {
+                                 double T, int r, double* front, unsigned long long* evals,
+                                 unsigned long long* vk) {
   const GridDesc& g = P.g;
   const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
   // last evaluated value, still valid while nothing the node reads has changed
@@ -165,6 +170,7 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     const double tv = __ldcg(a.rs.tent + gbase + l);
     if (tv > T) {
       *front = tv;
+      vk[0]++;
       return 1u << DIR_SELF;
     }
   }
@@ -173,7 +179,10 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   double Lold;
   int dold;
   node_key(P, l, told, cb, &Lold, &dold);
-  if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) return 0;  // source points are fixed
+  if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) {  // source points are fixed
+    vk[1]++;
+    return 0;
+  }
   // immediate neighbours: potential (the smallest of their traveltimes)
   double t1[ND][2];
   long long l1[ND][2];
@@ -192,7 +201,10 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
       t1[ax][s] = __ldcg(P.t + l1[ax][s]);
       pot = fmin(pot, t1[ax][s]);
     }
-  if (!(pot < EIK_INF)) return 0;  // nothing reached around it yet
+  if (!(pot < EIK_INF)) {  // nothing reached around it yet
+    vk[2]++;
+    return 0;
+  }
   Nbhd nb;
   nb_clear(nb);
   node_dh(g, c[0], nb.dh);
@@ -206,6 +218,7 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * nb.slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
   if (lb > T) {
     *front = lb;
+    vk[3]++;
     return 1u << DIR_SELF;
   }
   // from here the node is evaluated with the neighbours' current values: a change after
@@ -249,10 +262,12 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   a.rs.tent[gbase + l] = nv;
   if (!tkchange) {
     if (ncb != cb) P.code[l] = ncb;
+    vk[5]++;
     return 0;
   }
   if (nv > T) {  // not final yet: keep the old value and come back when the front is there
     *front = nv;
+    vk[4]++;
     return 1u << DIR_SELF;
   }
   P.t[l] = nv;
@@ -276,6 +291,13 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     int p[3] = {c[0], c[1], c[2]};
     p[ax] += off;
     const long long lj = lin3(g, p[0], p[1], p[2]);
+    if (off == 2 || off == -2) {
+      // the node two steps away reads this one only through the node in between, which
+      // must be reached first; when it is, its own change lists that node
+      int m[3] = {c[0], c[1], c[2]};
+      m[ax] += off / 2;
+      if (!(__ldcg(P.t + lin3(g, m[0], m[1], m[2])) < EIK_INF)) continue;
+    }
     if (*(volatile int32_t*)(a.rs.stamp + gbase + lj) < r) {
       const double tj = __ldcg(P.t + lj);
       double Lj;
@@ -287,7 +309,8 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     a.rs.dirty[gbase + lj] = 1;
     dirs |= 1u << k;
   }
-  *front = nv;
+  *front = nv + P.incmin;  // no node reading this one can get a smaller value from it
+  vk[6]++;
   return dirs;
 }
 
@@ -299,10 +322,14 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
 // key changed lists the nodes whose stencil reads it for the next round; a node below the
 // front is listed again. The result is the same fixed point as any other evaluation order.
 template <int ND>
-__global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_rounds_kernel(SolveArgs a) {
+#ifndef EIK_FWD_MINBLOCKS
+#define EIK_FWD_MINBLOCKS 4  // CTAs per SM the register budget is sized for
+#endif
+__global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_rounds_kernel(SolveArgs a) {
   const int lane = threadIdx.x & 31;
   const unsigned long long N = (unsigned long long)npts(a.probs[0].g);  // every problem has the same grid
   unsigned long long evals = 0;
+  unsigned long long vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
   int r = 0;
   for (; r < a.rs.max_rounds; r++) {
     const int b3 = r % 3, nb3 = (r + 1) % 3;
@@ -313,6 +340,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_rounds_kernel(SolveAr
     unsigned int* Lnext = a.rs.list[(r + 1) & 1];
     const unsigned long long* nm = a.rs.nextmin + (size_t)b3 * a.nprob;
     unsigned long long* nmn = a.rs.nextmin + (size_t)nb3 * a.nprob;
+    const double* thr_prev = a.rs.thr + (size_t)((r + 1) & 1) * a.nprob;  // thresholds of round r-1
+    double* thr_cur = a.rs.thr + (size_t)(r & 1) * a.nprob;
+    if (blockIdx.x == 0)
+      for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
+        thr_cur[p] = fmax(thr_prev[p], __longlong_as_double((long long)ld_volatile(nm + p)) + a.probs[p].delta);
     for (;;) {
       unsigned int base = 0;
       if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
@@ -328,10 +360,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_rounds_kernel(SolveAr
         prob = (int)(gid / N);
         l = (long long)(gid - (unsigned long long)prob * N);
         const CoarseProblem& P = a.probs[prob];
-        const double T = __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta;
+        // window of one round width above the smallest pending front, never moving back
+        const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
         const unsigned long long gb = (unsigned long long)prob * N;
-        dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals)
-                         : process_node<2>(a, P, gb, l, T, r, &front, &evals);
+        dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
+                         : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
       }
       // list the next round's nodes once each (per-node round stamps)
       const CoarseProblem& P = a.probs[prob];
@@ -388,6 +421,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 2) coarse_rounds_kernel(SolveAr
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
   if (lane == 0 && evals) atomicAdd(a.node_evals, evals);
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    unsigned long long v = vk[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && v) atomicAdd(a.rs.visits + k, v);
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *a.rs.rounds = r;
     if (r >= a.rs.max_rounds) {

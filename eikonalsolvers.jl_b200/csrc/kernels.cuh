@@ -65,6 +65,7 @@ struct CoarseProblem {
   long long tbase; // first global tile id of this problem
   double tinv;     // QBUCKETS / (time scale of this problem): trigger time -> bucket
   double delta;    // round width of the forward solve (traveltime units)
+  double incmin;   // smallest increment of the local update over a neighbour: (2/3) h s_min / sqrt(nd)
 };
 
 // Bucketed priority queue of tile ids: QBUCKETS bounded multi-producer/multi-consumer
@@ -90,8 +91,10 @@ struct RoundState {
   unsigned int* cnt;            // [3] list length per round (mod 3)
   unsigned int* grab;           // [3] next list entry to take per round (mod 3)
   unsigned long long* nextmin;  // [3][nprob] smallest pending potential (double bits)
+  double* thr;                  // [2][nprob] threshold of the previous / current round
   unsigned int* bar;            // [2] grid barrier: arrivals, generation
   int32_t* rounds;              // rounds run
+  unsigned long long* visits;   // [7] outcomes of the forward's list visits
   int32_t max_rounds;
 };
 

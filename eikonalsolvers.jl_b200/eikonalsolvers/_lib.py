@@ -13,7 +13,8 @@ import threading
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(os.path.dirname(_HERE), "lib", "libeikcuda.so")
+# EIKCUDA_LIB points at another build of the library (for example a tuning variant)
+LIBPATH = os.environ.get("EIKCUDA_LIB") or os.path.join(os.path.dirname(_HERE), "lib", "libeikcuda.so")
 
 EIK_OK = 0
 ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EIK_ERR_NOT_CONVERGED",
@@ -51,7 +52,8 @@ class eik_stats(C.Structure):
     _fields_ = [("warn_mask", C.c_uint32), ("err_mask", C.c_uint32), ("tile_activations", C.c_uint64),
                 ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
                 ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_rounds", C.c_uint64),
-                ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64)]
+                ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64),
+                ("fwd_visits", C.c_uint64 * 7)]
 
 
 _lib = None

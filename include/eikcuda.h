@@ -102,6 +102,9 @@ typedef struct {
   uint64_t adj_rounds;       /* rounds of the adjoint sweep */
   uint64_t launches;         /* kernels this call launched */
   uint64_t fwd_rounds;       /* rounds of the forward solve */
+  uint64_t fwd_visits[7];    /* forward list visits by outcome: value cached above the front,
+                                source point, nothing reached, bound above the front,
+                                evaluated above the front, evaluated unchanged, changed */
 } eik_stats;
 
 /* Fills the reference defaults of ExtraParams(). */
