@@ -73,7 +73,7 @@ struct eik_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // whole call
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
-  double round_gate = 1.0;  // forward round width in units of (smallest spacing x smallest slowness)
+  double round_gate = 2.0;  // forward round width in units of (smallest spacing x smallest slowness)
   std::mutex mu;
   eik::Scratch scratch;
   size_t model_bytes = 0;

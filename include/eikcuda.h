@@ -120,7 +120,7 @@ const char* eik_last_error(eik_ctx* ctx);
 void* eik_ctx_stream(eik_ctx* ctx);
 /* Scheduling parameters of a context (results do not depend on them, only the amount of
  * work does): "round_gate" = width of a forward round in units of (smallest node spacing x
- * smallest slowness), default 1. Returns EIK_ERR_ASSERT for an unknown name or a value
+ * smallest slowness), default 2. Returns EIK_ERR_ASSERT for an unknown name or a value
  * out of range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 
