@@ -1030,7 +1030,7 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   ra.dpsi = dpsi;
   adj_recv_kernel<<<(int)((nsrc + 63) / 64), 64, 0, st>>>(ra);
   cudaEventRecord(ctx->evk[4], st);
-  CUDA_OK(ctx, nd == 3 ? launch_adj_solve<3>(aa, ctx->nsm, st) : launch_adj_solve<2>(aa, ctx->nsm, st));
+  CUDA_OK(ctx, nd == 3 ? launch_adj_solve<3>(aa, ctx->solve_sms(), st) : launch_adj_solve<2>(aa, ctx->solve_sms(), st));
   cudaEventRecord(ctx->evk[5], st);
   adj_check_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, N, fw.fb.err);
   CUDA_OK(ctx, cudaGetLastError());

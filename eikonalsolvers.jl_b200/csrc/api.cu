@@ -367,7 +367,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
   CUDA_OK(ctx, cudaGetLastError());
   cudaEventRecord(ctx->evk[2], st);
-  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->nsm, st));
+  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->solve_sms(), st));
   cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
   fw->fb = fb;
@@ -480,6 +480,11 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
   if (std::strcmp(name, "round_gate") == 0) {
     if (!(value > 0.0 && value < 1e6)) return fail(ctx, EIK_ERR_ASSERT, "round_gate must be in (0, 1e6)");
     ctx->round_gate = value;
+    return EIK_OK;
+  }
+  if (std::strcmp(name, "sm_fraction") == 0) {
+    if (!(value > 0.0 && value <= 1.0)) return fail(ctx, EIK_ERR_ASSERT, "sm_fraction must be in (0, 1]");
+    ctx->sm_fraction = value;
     return EIK_OK;
   }
   return fail(ctx, EIK_ERR_ASSERT, "unknown parameter '%s'", name);

@@ -74,6 +74,11 @@ struct eik_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // whole call
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
   double round_gate = 2.0;  // forward round width in units of (smallest spacing x smallest slowness)
+  double sm_fraction = 1.0; // share of the SMs the persistent (cooperative) solves of this context use
+  int solve_sms() const {
+    const int n = (int)(sm_fraction * (double)nsm + 0.5);
+    return n < 1 ? 1 : (n > nsm ? nsm : n);
+  }
   std::mutex mu;
   eik::Scratch scratch;
   size_t model_bytes = 0;

@@ -204,3 +204,58 @@ def cfg4(scale: float = 1.0, nsrc: int = 48, forward=None) -> Workload:
     if forward is not None:
         w.pickobs, w.stdobs = _observations(vel, grd, coordsrc, coordrec, w.extraparams, 0.05, 13, forward)
     return w
+
+
+def serving_requests(n: int, rate: float, seed: int = 9, scale: float = 1.0, nmodels: int = 6,
+                     max_sources: int = 64):
+    """The serving mix: `n` requests with Poisson arrivals at `rate` per second over a pool
+    of `nmodels` resident models. 60 % 2D Cartesian (side U[128, 1024] nodes), 40 % 3D
+    Cartesian (side U[64, 192]); velocity a linear gradient (cfg1 style) or a correlated
+    random field (cfg2 style), half each; nsrc ~ U{1..max_sources}; 70 % eiktraveltime, 30 %
+    eikgradient :gradvel with observations from a 3 %-faster model plus N(0, 0.01^2).
+    `scale` shrinks the sides (tests). Returns (models, requests): models maps a key to
+    (vel, grd, vel_obs); every request is a dict with its arrival offset in seconds."""
+    rng = np.random.default_rng(seed)
+    models = {}
+    for m in range(nmodels):
+        three_d = rng.uniform() < 0.4
+        if three_d:
+            side = max(8, int(rng.integers(64, 193) * scale))
+            shape = (side, side, side)
+            h = 0.1
+            grd = Grid3DCart(hgrid=h, cooinit=(0.0, 0.0, 0.0), grsize=shape)
+        else:
+            side = max(8, int(rng.integers(128, 1025) * scale))
+            shape = (side, max(8, (side * 5) // 8))
+            h = 0.25
+            grd = Grid2DCart(hgrid=h, cooinit=(0.0, 0.0), grsize=shape)
+        if rng.uniform() < 0.5:
+            depth = np.arange(1, shape[-1] + 1, dtype=np.float64)
+            vel = np.broadcast_to(2.5 + 2.5 * depth / shape[-1], shape).copy()
+        else:
+            f = gaussian_random_field(shape, 4.0 if scale < 1 else 20.0, seed=int(rng.integers(1 << 30)))
+            vel = 2.0 + 3.0 * _normal_cdf(f)
+        models[f"m{m}"] = (np.ascontiguousarray(vel), grd, np.ascontiguousarray(vel * 1.03))
+    keys = list(models)
+    t = 0.0
+    reqs = []
+    for i in range(n):
+        t += rng.exponential(1.0 / rate)
+        key = keys[int(rng.integers(len(keys)))]
+        vel, grd, _ = models[key]
+        nd = grd.ndim
+        ns = int(rng.integers(1, max_sources + 1))
+        ext = [float(grd.cooinit[d] + (grd.grsize[d] - 1) * grd.spacing[d]) for d in range(nd)]
+        cs = np.array([[_avoid_node_and_half(rng.uniform(0.1 * e, 0.9 * e), grd.spacing[d], rng)
+                        for d, e in enumerate(ext)] for _ in range(ns)])
+        nr = 10
+        rec = np.column_stack([np.linspace(0.0, ext[0], nr)] + [np.full(nr, 0.5 * ext[d]) for d in range(1, nd - 1)]
+                              + [np.zeros(nr)])
+        kind = "traveltime" if rng.uniform() < 0.7 else "gradient"
+        r = dict(t=t, model=key, kind=kind, coordsrc=cs, coordrec=[rec.copy() for _ in range(ns)])
+        if kind == "gradient":  # straight-ray times at the mean velocity, plus noise
+            vm = float(np.mean(vel))
+            r["pickobs"] = [np.linalg.norm(rec - cs[k], axis=1) / vm + rng.normal(0.0, 0.01, nr) for k in range(ns)]
+            r["stdobs"] = [np.full(nr, 0.01) for _ in range(ns)]
+        reqs.append(r)
+    return models, reqs

@@ -120,8 +120,10 @@ const char* eik_last_error(eik_ctx* ctx);
 void* eik_ctx_stream(eik_ctx* ctx);
 /* Scheduling parameters of a context (results do not depend on them, only the amount of
  * work does): "round_gate" = width of a forward round in units of (smallest node spacing x
- * smallest slowness), default 2. Returns EIK_ERR_ASSERT for an unknown name or a value
- * out of range. */
+ * smallest slowness), default 2; "sm_fraction" = share of the SMs that the persistent
+ * solve kernels of this context occupy, in (0, 1], default 1 (contexts whose calls overlap
+ * on one GPU, as in a serving loop, each take a share so that their solves can be resident
+ * together). Returns EIK_ERR_ASSERT for an unknown name or a value out of range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 
 /* Uploads a velocity model (host, column-major, FP64) and keeps it resident. Checks

@@ -1,0 +1,78 @@
+"""Two ranks on CPU (gloo): the sharded gradient equals the reference's :sharedmem gradient
+with two threads (each rank solves one distribsrcs group, here with the oracle as the local
+solver), and the shard ranges are distribsrcs' groups."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from eikonalsolvers.parallel import distribsrcs, shard
+
+
+def test_distribsrcs_groups():
+    assert distribsrcs(7, 3) == [(0, 2), (3, 4), (5, 6)]
+    assert distribsrcs(2, 4) == [(0, 0), (1, 1)]
+    assert shard(7, 3, 1) == (3, 5) and shard(2, 4, 3) is None
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank(rank, world, port, case, out):
+    import torch.distributed as dist
+    import eikoracle as O
+    from eikonalsolvers.parallel import eikgradient_sharded
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    vel, grd, cs, rec, po, so, ep = case
+
+    def local(v, g, c, r, p, s, wg, e):
+        return O.eikgradient(v, g, c, r, p, s, wg, extraparams=e)
+    res = eikgradient_sharded(vel, grd, cs, rec, po, so, "gradvelandsrcloc", ep, local=local)
+    out[rank] = res
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_gradient_equals_sharedmem_groups():
+    import eikoracle as O
+    from eikonalsolvers import ExtraParams
+    from eikonalsolvers import configs as CF
+    w = CF.cfg2(scale=0.125, nsrc=2)
+    h = w.grd.hgrid
+    x0 = w.coordsrc[0][0]
+    cs = np.array([[x0 + 0.37 * h * k, (60 - 6.3 * k) * h + 0.011] for k in range(5)])  # stacked: carry-over matters
+    rec = [w.coordrec[0]] * 5
+    ep = ExtraParams(radiussmoothgradsrc=0)
+    po = O.eiktraveltime(w.vel * 1.02, w.grd, cs, rec, extraparams=ep)
+    so = [0.01 * np.ones(p.shape) for p in po]
+    case = (w.vel, w.grd, cs, rec, po, so, ep)
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as man:
+        out = man.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_rank, args=(r, 2, port, case, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(timeout=300)
+        assert all(p.exitcode == 0 for p in procs)
+        res = dict(out)
+    eps = ExtraParams(radiussmoothgradsrc=0, parallelkind="sharedmem")
+    gv, gs, m = O.eikgradient(w.vel, w.grd, cs, rec, po, so, "gradvelandsrcloc", extraparams=eps, nthreads=2)
+    gv1, gs1, m1 = O.eikgradient(w.vel, w.grd, cs, rec, po, so, "gradvelandsrcloc", extraparams=ep)
+    assert np.linalg.norm(gv - gv1) > 1e-6 * np.linalg.norm(gv)  # the grouping is visible
+    for r in range(2):
+        g, s, mm = res[r]
+        assert np.array_equal(g, gv)
+        assert np.array_equal(s, gs)
+        assert mm == m

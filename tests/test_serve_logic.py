@@ -1,0 +1,104 @@
+"""CPU tests of the serving loop's host logic (admission order, batching of traveltime
+requests on one model, splitting of results, failure isolation), with a stand-in for the
+device context that records the calls it receives."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from eikonalsolvers import Grid2DCart
+from eikonalsolvers.serve import Request, Server
+
+
+class FakeContext:
+    """Answers traveltime with picks = source x-coordinate + receiver index, gradient with
+    a field of the source count; records every call."""
+    calls = []
+    lock = threading.Lock()
+
+    def __init__(self):
+        self.params = {}
+        self.next_id = 0
+
+    def set_param(self, k, v):
+        self.params[k] = v
+
+    def upload(self, vel, grd):
+        self.next_id += 1
+        return self.next_id
+
+    def release(self, mid):
+        pass
+
+    def close(self):
+        pass
+
+    def traveltime(self, mid, grd, cs, recs, extraparams=None):
+        time.sleep(0.01)
+        with self.lock:
+            self.calls.append(("traveltime", len(cs)))
+        return [cs[s][0] + np.arange(len(recs[s]), dtype=float) for s in range(len(cs))]
+
+    def gradient(self, mid, grd, cs, recs, po, so, which, extraparams=None):
+        time.sleep(0.01)
+        if np.any(np.isnan(cs)):
+            raise RuntimeError("bad source")
+        with self.lock:
+            self.calls.append(("gradient", len(cs)))
+        return np.full(grd.grsize, float(len(cs))), 1.0
+
+
+@pytest.fixture
+def grd():
+    return Grid2DCart(hgrid=1.0, cooinit=(0.0, 0.0), grsize=(8, 8))
+
+
+def _req(kind, xs, model="a"):
+    cs = np.array([[x, 1.0] for x in xs])
+    recs = [np.zeros((3, 2)) for _ in xs]
+    return Request(model=model, kind=kind, coordsrc=cs, coordrec=recs,
+                   pickobs=[np.zeros(3)] * len(xs), stdobs=[np.ones(3)] * len(xs))
+
+
+def test_traveltime_requests_on_one_model_are_batched_and_split(grd):
+    FakeContext.calls = []
+    srv = Server(slots=1, max_batch_sources=10, context_factory=FakeContext)
+    srv.register_model("a", np.ones(grd.grsize), grd)
+    srv.register_model("b", np.ones(grd.grsize), grd)
+    blocker = srv.submit(_req("gradient", [9.0]))  # keeps the only slot busy
+    futs = [srv.submit(_req("traveltime", [1.0, 2.0])), srv.submit(_req("traveltime", [3.0], model="b")),
+            srv.submit(_req("traveltime", [4.0, 5.0, 6.0]))]
+    blocker.result(timeout=10)
+    res = [f.result(timeout=10) for f in futs]
+    srv.close()
+    assert [float(p[0]) for p in res[0]] == [1.0, 2.0]
+    assert [float(p[0]) for p in res[2]] == [4.0, 5.0, 6.0]
+    assert [float(p[0]) for p in res[1]] == [3.0]
+    # the two requests on model "a" ran as one call of 5 sources, "b" alone
+    assert ("traveltime", 5) in FakeContext.calls and ("traveltime", 1) in FakeContext.calls
+    st = srv.stats()
+    assert st["requests"] == 4 and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_gradient_requests_are_never_merged_and_failures_stay_local(grd):
+    FakeContext.calls = []
+    srv = Server(slots=2, context_factory=FakeContext)
+    srv.register_model("a", np.ones(grd.grsize), grd)
+    good = [srv.submit(_req("gradient", [1.0, 2.0])) for _ in range(3)]
+    bad = srv.submit(_req("gradient", [np.nan]))
+    for f in good:
+        g, m = f.result(timeout=10)
+        assert g[0, 0] == 2.0
+    with pytest.raises(RuntimeError, match="bad source"):
+        bad.result(timeout=10)
+    srv.close()
+    assert FakeContext.calls.count(("gradient", 2)) == 3
+
+
+def test_slots_get_an_sm_share_and_unknown_models_are_refused(grd):
+    srv = Server(slots=4, context_factory=FakeContext)
+    assert all(c.params["sm_fraction"] == 0.25 for c in srv._ctx)
+    with pytest.raises(KeyError):
+        srv.submit(_req("traveltime", [1.0], model="zzz"))
+    srv.close()
