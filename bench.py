@@ -57,6 +57,11 @@ def parse():
                     help="sources timed one per call for the plain path (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--serve-requests", type=int, default=30,
+                    help="requests of the serving leg (Poisson arrivals; 0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="arrival rate of the serving leg, req/s")
+    ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="grid scale of the serving mix")
     return ap.parse_args()
 
 
@@ -367,7 +372,7 @@ def main_b200(args):
 
     # ---- roofline of the dominant kernel (measured inside the timed region)
     peak, peak_kind = measured_peaks()
-    kern = {"coarse_solve_kernel": (solve_ms, 16), "adj_solve_kernel": (adj_ms, 16),
+    kern = {"coarse_rounds_kernel": (solve_ms, 16), "adj_rounds_kernel": (adj_ms, 16),
             "fine_fmm_kernel": (fine_ms, 16)}
     top = max(kern, key=lambda k: kern[k][0])
     kms, bpn = kern[top]
@@ -409,15 +414,57 @@ def main_b200(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "serve": None,
             "stats": {"tile_activations": int(st.tile_activations), "node_evals": int(st.node_evals),
                       "adj_rounds": int(st.adj_rounds), "fwd_rounds": int(st.fwd_rounds), "evals_per_node": st.node_evals / (N * nsrc)},
         }
-        print(json.dumps(line), flush=True)
     ctx.release(mid)
     ctx.close()
+    if rank == 0:
+        if ws == 1 and args.serve_requests > 0:
+            try:
+                line["serve"] = run_serve_leg(args, local)
+            except Exception as e:
+                line["serve"] = {"error": str(e)}
+        print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_serve_leg(args, device):
+    """Serving mix (2D/3D Cartesian models resident on the device, 70 % traveltime / 30 %
+    gradient requests with 1-64 sources) arriving as a Poisson process; latency from
+    submission to result, on the host clock."""
+    from eikonalsolvers import configs as CF
+    from eikonalsolvers.serve import Request, Server
+    models, reqs = CF.serving_requests(n=args.serve_requests, rate=args.serve_rate, seed=9, scale=args.serve_scale)
+    with Server(device=device, slots=args.serve_slots) as srv:
+        for k, (vel, grd, _) in models.items():
+            srv.register_model(k, vel, grd)
+        # warm each slot on every model (uploads, scratch growth) before the clock starts
+        centre = lambda g: np.array([[0.5 * (g.grsize[d] - 1) * g.spacing[d] + 1e-3 for d in range(g.ndim)]])  # noqa: E731
+        warm = [srv.submit(Request(model=k, kind="traveltime", coordsrc=centre(g), coordrec=[np.zeros((1, g.ndim))]))
+                for k, (v, g, _) in models.items() for _ in range(args.serve_slots)]
+        for f in warm:
+            f.result()
+        srv._done.clear()
+        t0 = time.perf_counter()
+        futs = []
+        for r in reqs:
+            delay = t0 + r["t"] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            futs.append(srv.submit(Request(model=r["model"], kind=r["kind"], coordsrc=r["coordsrc"],
+                                           coordrec=r["coordrec"], pickobs=r.get("pickobs"),
+                                           stdobs=r.get("stdobs"))))
+        for f in futs:
+            f.result()
+        st = srv.stats()
+    st.update({"offered_rate_req_s": args.serve_rate, "slots": args.serve_slots,
+               "mix": "seeded: 60% 2D side 128-1024, 40% 3D side 64-192, 1-64 sources, 70% traveltime / "
+                      "30% gradvel, 6 resident models"})
+    return st
 
 
 def main_reference(args):

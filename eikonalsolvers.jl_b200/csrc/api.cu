@@ -317,11 +317,6 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   const unsigned long long want = std::max<unsigned long long>((unsigned long long)sa.ntiles / 16, 1ull << 16);
   while (cap < want) cap <<= 1;
   sa.q.mask = cap - 1;
-  GET(sa.tile_faces, uint32_t, "tile_faces", sa.ntiles);
-  GET(sa.tile_flag, int32_t, "tile_flag", sa.ntiles);
-  GET(sa.q.items, unsigned long long, "q_items", cap * QBUCKETS);
-  GET(sa.q.seq, unsigned long long, "q_seq", cap * QBUCKETS);
-  GET(sa.tile_prio, unsigned long long, "tile_prio", sa.ntiles);
   unsigned long long* ctr;
   GET(ctr, unsigned long long, "q_ctr", 2 * QBUCKETS + 8);
   sa.q.head = ctr;
@@ -330,13 +325,15 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   sa.node_evals = ctr + 2 * QBUCKETS + 1;
   sa.pending = (int32_t*)(ctr + 2 * QBUCKETS + 2);
   sa.abort_flag = (int32_t*)(ctr + 2 * QBUCKETS + 3);
-  if ((unsigned long long)nsrc * (unsigned long long)N >= (1ull << 32))
+  // round-solver state, shared by the refined windows' solve and the coarse solve
+  const long long rsn = nsrc * std::max<long long>(N, refine ? fb.nfmax : 1);
+  if ((unsigned long long)rsn >= (1ull << 32))
     return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "more than 2^32 node-sources in one call: split the sources");
-  GET(sa.rs.stamp, int32_t, "rs_stamp", nsrc * N);
-  GET(sa.rs.tent, double, "rs_tent", nsrc * N);
-  GET(sa.rs.dirty, uint8_t, "rs_dirty", nsrc * N);
-  GET(sa.rs.list[0], unsigned int, "rs_list0", nsrc * N);
-  GET(sa.rs.list[1], unsigned int, "rs_list1", nsrc * N);
+  GET(sa.rs.stamp, int32_t, "rs_stamp", rsn);
+  GET(sa.rs.tent, double, "rs_tent", rsn);
+  GET(sa.rs.dirty, uint8_t, "rs_dirty", rsn);
+  GET(sa.rs.list[0], unsigned int, "rs_list0", rsn);
+  GET(sa.rs.list[1], unsigned int, "rs_list1", rsn);
   GET(sa.rs.nextmin, unsigned long long, "rs_nextmin", 3 * nsrc);
   GET(sa.rs.thr, double, "rs_thr", 2 * nsrc);
   {
@@ -349,19 +346,66 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     sa.rs.visits = reinterpret_cast<unsigned long long*>(rc32 + 12);  // 8-byte aligned: 7 counters
   }
   sa.rs.max_rounds = 1 << 24;
+  sa.rs.stride = (unsigned long long)N;
   sa.err = fb.err;
   sa.probs = dp;
   sa.max_activations = 400ull * (unsigned long long)sa.ntiles + 100000ull;
   sa.max_passes = 4096;
   sa.gate = 1.0;
   sa.timeout_ns = 20LL * 1000 * 1000 * 1000;
+  // refined windows: one more round-solver problem per source
+  CoarseProblem* fprobs = nullptr;
+  int32_t* fseed_lin = nullptr;
+  double *fseed_tt = nullptr, *fslow = nullptr, *fkL = nullptr;
+  uint8_t *fkd = nullptr, *ftie = nullptr;
+  if (refine) {
+    GET(fprobs, CoarseProblem, "fine_probs", nsrc);
+    GET(fseed_lin, int32_t, "fine_seed_lin", nsrc * 8);
+    GET(fseed_tt, double, "fine_seed_tt", nsrc * 8);
+    GET(fslow, double, "fine_slow", nsrc * fb.nfmax);
+    GET(fkL, double, "fine_kL", nsrc * fb.nfmax);
+    GET(fkd, uint8_t, "fine_kd", nsrc * fb.nfmax);
+    GET(ftie, uint8_t, "fine_tie", nsrc);
+  }
 #undef GET
   CUDA_OK(ctx, cudaMemcpyAsync(dp, hp.data(), sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.err, 0, sizeof(uint32_t) * 4, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.out, 0, sizeof(SrcOut) * nsrc, st));
   cudaEventRecord(ctx->evk[0], st);
-  if (refine) launch_fine(fb, st);
-  else launch_srcbox(fb, st);
+  int nlaunch = 5;  // start-up, init, round init, seeds, solve
+  if (refine && ctx->fine_replay) {
+    launch_fine(fb, st);
+  } else if (refine) {
+    // the windows as round-solver problems, then the heap's stop reconstructed from keys
+    launch_fine_setup(fb, fprobs, m.smin, ctx->round_gate, fseed_lin, fseed_tt, fslow, fkL, fkd, st);
+    SolveArgs fsa = sa;
+    fsa.probs = fprobs;
+    fsa.rs.stride = (unsigned long long)fb.nfmax;
+    fsa.activations = sa.activations + 6;  // own counters: the coarse solve's stay separate
+    fsa.node_evals = sa.activations + 7;
+    launch_rounds_init(fsa, st);
+    launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
+    CUDA_OK(ctx, launch_coarse_solve(fsa, ctx->solve_sms(), st));
+    launch_fine_select(fb, fprobs, ftie, st);
+    CUDA_OK(ctx, cudaGetLastError());
+    std::vector<uint8_t> tie(nsrc);
+    CUDA_OK(ctx, cudaMemcpyAsync(tie.data(), ftie, nsrc, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(ctx, cudaStreamSynchronize(st));
+    std::vector<int32_t> list;
+    for (int64_t s = 0; s < nsrc; s++)
+      if (tie[s]) list.push_back((int32_t)s);
+    nlaunch += 6;
+    if (!list.empty()) {  // stops decided by exact ties: replay the heap for those sources
+      int32_t* dlist = (int32_t*)S.get("fine_replay_list", sizeof(int32_t) * list.size(), &rc);
+      if (!dlist) return fail(ctx, rc, "scratch allocation failed");
+      CUDA_OK(ctx, cudaMemcpyAsync(dlist, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, st));
+      launch_fine_replay(fb, dlist, (int)list.size(), st);
+      nlaunch += 1;
+    }
+    if (stats) stats->fine_replays += list.size();
+  } else {
+    launch_srcbox(fb, st);
+  }
   cudaEventRecord(ctx->evk[1], st);
   CUDA_OK(ctx, cudaGetLastError());
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
@@ -378,7 +422,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   fw->kd = kd;
   fw->N = N;
   fw->nsrc = nsrc;
-  if (stats) stats->launches += 5;  // start-up, init, queue init, seeds, solve
+  if (stats) stats->launches += nlaunch;
   return EIK_OK;
 }
 
@@ -480,6 +524,10 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
   if (std::strcmp(name, "round_gate") == 0) {
     if (!(value > 0.0 && value < 1e6)) return fail(ctx, EIK_ERR_ASSERT, "round_gate must be in (0, 1e6)");
     ctx->round_gate = value;
+    return EIK_OK;
+  }
+  if (std::strcmp(name, "fine_replay") == 0) {
+    ctx->fine_replay = value != 0.0;
     return EIK_OK;
   }
   if (std::strcmp(name, "sm_fraction") == 0) {

@@ -63,7 +63,7 @@ __global__ void queue_init_kernel(SolveArgs a) {
 
 
 __global__ void rounds_init_kernel(SolveArgs a) {
-  const long long tot = npts(a.probs[0].g) * a.nprob;
+  const long long tot = (long long)a.rs.stride * a.nprob;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
        q += (long long)gridDim.x * blockDim.x) {
     a.rs.stamp[q] = -1;
@@ -91,17 +91,18 @@ __global__ void rounds_init_kernel(SolveArgs a) {
   }
 }
 
-// Seeds: fixed traveltimes of the source points (coarse source box or coarse-coincident
-// accepted fine nodes); the tiles within two nodes of a seed start round 0, whose
-// threshold is based on the smallest seed traveltime.
+// Seeds: fixed traveltimes of the source points (coarse source box, coarse-coincident
+// accepted fine nodes, or the source box of a refined window); the nodes within two steps
+// of a seed start round 0, whose threshold is based on the smallest seed traveltime.
 template <int ND>
-__global__ void seed_kernel(SolveArgs a, ForwardBatch fb) {
+__global__ void seed_kernel(SolveArgs a, const int32_t* seed_lin, const double* seed_tt, const SrcOut* out,
+                            int fine_corners, int seedcap) {
   const int s = blockIdx.x;
   const CoarseProblem& P = a.probs[s];
-  const int ns = fb.out[s].nseeds;
+  const int ns = fine_corners ? out[s].nsrcf : out[s].nseeds;
   for (int q = threadIdx.x; q < ns; q += blockDim.x) {
-    const long long l = fb.seed_lin[(size_t)s * fb.seedcap + q];
-    P.t[l] = fb.seed_tt[(size_t)s * fb.seedcap + q];
+    const long long l = seed_lin[(size_t)s * seedcap + q];
+    P.t[l] = seed_tt[(size_t)s * seedcap + q];
     P.code[l] = (uint8_t)(CODE_NONE | CODE_SRC_BIT);
     P.kL[l] = -EIK_INF;
     P.kd[l] = 0;
@@ -109,14 +110,14 @@ __global__ void seed_kernel(SolveArgs a, ForwardBatch fb) {
   __syncthreads();
   __threadfence();
   for (int q = threadIdx.x; q < ns; q += blockDim.x) {
-    const long long l = fb.seed_lin[(size_t)s * fb.seedcap + q];
+    const long long l = seed_lin[(size_t)s * seedcap + q];
     const int i = (int)(l % P.g.n[0]);
     const int j = (int)((l / P.g.n[0]) % P.g.n[1]);
     const int k = (int)(l / ((long long)P.g.n[0] * P.g.n[1]));
     const int c[3] = {i, j, k};
-    const double tt = fb.seed_tt[(size_t)s * fb.seedcap + q];
+    const double tt = seed_tt[(size_t)s * seedcap + q];
     if (tt < EIK_INF) atomicMin(a.rs.nextmin + s, (unsigned long long)__double_as_longlong(tt));
-    const unsigned long long gbase = (unsigned long long)s * (unsigned long long)npts(P.g);
+    const unsigned long long gbase = (unsigned long long)s * a.rs.stride;
     for (int ax = 0; ax < ND; ax++)
       for (int d = -2; d <= 2; d++) {
         if (d == 0) continue;
@@ -327,7 +328,7 @@ template <int ND>
 #endif
 __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_rounds_kernel(SolveArgs a) {
   const int lane = threadIdx.x & 31;
-  const unsigned long long N = (unsigned long long)npts(a.probs[0].g);  // every problem has the same grid
+  const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
   unsigned long long evals = 0;
   unsigned long long vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
   int r = 0;
@@ -490,8 +491,15 @@ void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs
   const long long N = npts(hprobs[0].g);
   coarse_init_kernel<<<1184, 256, 0, st>>>(dprobs, nprob, N);
   rounds_init_kernel<<<296, 256, 0, st>>>(sa);
-  if (sa.nd == 3) seed_kernel<3><<<nprob, 128, 0, st>>>(sa, fb);
-  else seed_kernel<2><<<nprob, 128, 0, st>>>(sa, fb);
+  launch_rounds_seed(sa, fb.seed_lin, fb.seed_tt, fb.out, false, fb.seedcap, st);
+}
+
+void launch_rounds_init(const SolveArgs& sa, cudaStream_t st) { rounds_init_kernel<<<296, 256, 0, st>>>(sa); }
+
+void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const double* seed_tt, const SrcOut* out,
+                        bool fine_corners, int seedcap, cudaStream_t st) {
+  if (sa.nd == 3) seed_kernel<3><<<sa.nprob, 128, 0, st>>>(sa, seed_lin, seed_tt, out, fine_corners ? 1 : 0, seedcap);
+  else seed_kernel<2><<<sa.nprob, 128, 0, st>>>(sa, seed_lin, seed_tt, out, fine_corners ? 1 : 0, seedcap);
 }
 
 void launch_queue_init(const SolveArgs& sa, cudaStream_t st) { queue_init_kernel<<<296, 256, 0, st>>>(sa); }

@@ -93,6 +93,7 @@ struct RoundState {
   unsigned long long* nextmin;  // [3][nprob] smallest pending potential (double bits)
   double* thr;                  // [2][nprob] threshold of the previous / current round
   unsigned int* bar;            // [2] grid barrier: arrivals, generation
+  unsigned long long stride;    // node ids: problem * stride + node
   int32_t* rounds;              // rounds run
   unsigned long long* visits;   // [7] outcomes of the forward's list visits
   int32_t max_rounds;
@@ -127,6 +128,18 @@ void launch_fine(const ForwardBatch& fb, cudaStream_t st);
 size_t fine_smem_bytes(int heapcap);
 void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs, int nprob,
                         const ForwardBatch& fb, const SolveArgs& sa, cudaStream_t st);
+// Round-solver state reset, and seeding from per-problem seed lists (fixed values).
+void launch_rounds_init(const SolveArgs& sa, cudaStream_t st);
+void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const double* seed_tt, const SrcOut* out,
+                        bool fine_corners, int seedcap, cudaStream_t st);
+// Refined start-up as a fixed point: window set-up, the fine problems' arrays, the
+// acceptance set at the reference's stop, and the exact heap replay for the sources
+// whose stop is decided by a tie (flags in fine_tie, nonzero = replay needed).
+void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, double smin, double gate,
+                       int32_t* fseed_lin, double* fseed_tt, double* fine_slow, double* fine_kL, uint8_t* fine_kd,
+                       cudaStream_t st);
+void launch_fine_select(const ForwardBatch& fb, const CoarseProblem* fprobs, uint8_t* fine_tie, cudaStream_t st);
+void launch_fine_replay(const ForwardBatch& fb, const int32_t* srclist, int n, cudaStream_t st);
 cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
 void launch_queue_init(const SolveArgs& sa, cudaStream_t st);  // empty queue, idle tiles, zero counters
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,

@@ -75,6 +75,7 @@ struct eik_ctx {
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
   double round_gate = 2.0;  // forward round width in units of (smallest spacing x smallest slowness)
   double sm_fraction = 1.0; // share of the SMs the persistent (cooperative) solves of this context use
+  bool fine_replay = false; // refined start-up by exact heap replay for every source (else only on ties)
   int solve_sms() const {
     const int n = (int)(sm_fraction * (double)nsm + 0.5);
     return n < 1 ? 1 : (n > nsm ? nsm : n);

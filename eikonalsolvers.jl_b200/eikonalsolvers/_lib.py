@@ -53,7 +53,7 @@ class eik_stats(C.Structure):
                 ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
                 ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_rounds", C.c_uint64),
                 ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64),
-                ("fwd_visits", C.c_uint64 * 7)]
+                ("fine_replays", C.c_uint64), ("fwd_visits", C.c_uint64 * 7)]
 
 
 _lib = None

@@ -102,6 +102,7 @@ typedef struct {
   uint64_t adj_rounds;       /* rounds of the adjoint sweep */
   uint64_t launches;         /* kernels this call launched */
   uint64_t fwd_rounds;       /* rounds of the forward solve */
+  uint64_t fine_replays;      /* sources whose refined start-up needed the exact heap replay */
   uint64_t fwd_visits[7];    /* forward list visits by outcome: value cached above the front,
                                 source point, nothing reached, bound above the front,
                                 evaluated above the front, evaluated unchanged, changed */
@@ -123,7 +124,9 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * smallest slowness), default 2; "sm_fraction" = share of the SMs that the persistent
  * solve kernels of this context occupy, in (0, 1], default 1 (contexts whose calls overlap
  * on one GPU, as in a serving loop, each take a share so that their solves can be resident
- * together). Returns EIK_ERR_ASSERT for an unknown name or a value out of range. */
+ * together); "fine_replay" = 1 replays the refined start-up's heap for every source
+ * instead of only where an exact tie decides its stop (default 0). Returns
+ * EIK_ERR_ASSERT for an unknown name or a value out of range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 
 /* Uploads a velocity model (host, column-major, FP64) and keeps it resident. Checks
