@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libeikcuda.so")
 SOURCES = ["api.cu", "fine.cu", "coarse.cu", "adjoint.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "stencil.cuh", "kernels.cuh", "runtime.hpp", "queue.cuh", "rounds.cuh"]
+HEADERS = ["common.cuh", "stencil.cuh", "kernels.cuh", "runtime.hpp", "rounds.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false",
          "-std=c++17", "-Xcompiler", "-fPIC", "--cudart=static", "-Xptxas", "-v"]

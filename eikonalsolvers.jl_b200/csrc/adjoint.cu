@@ -14,7 +14,6 @@
 #include <vector>
 
 #include "../../include/eikcuda.h"
-#include "queue.cuh"
 #include "rounds.cuh"
 #include "runtime.hpp"
 

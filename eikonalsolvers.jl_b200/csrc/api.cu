@@ -185,15 +185,6 @@ int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev,
   CUDA_OK(ctx, cudaMemcpyAsync(&m.smin, dmin, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
   cudaFree(dflag);
-  {
-    // time scale for scheduling only: grid diagonal x mean slowness
-    double dh[3];
-    node_dh(m.g, m.g.n[0] / 2, dh);
-    double diag2 = 0.0;
-    for (int a = 0; a < m.g.nd; a++) diag2 += (double)m.g.n[a] * dh[a] * (double)m.g.n[a] * dh[a];
-    m.tscale = sqrt(diag2) * (ssum / (double)m.N);
-    if (!(m.tscale > 0.0) || !std::isfinite(m.tscale)) m.tscale = 1.0;
-  }
   if (nonpos) {
     cudaFree(m.vel);
     cudaFree(m.slow);
@@ -269,10 +260,6 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     GET(fb.fine_onh, uint8_t, "fine_onh", nsrc * fb.nfmax);
   }
   // coarse problems
-  using C3 = int;  // tile extents per dimensionality
-  const int TX = g.nd == 3 ? 4 : 8, TY = g.nd == 3 ? 4 : 8, TZ = g.nd == 3 ? 4 : 1;
-  const int nt[3] = {(g.n[0] + TX - 1) / TX, (g.n[1] + TY - 1) / TY, (g.n[2] + TZ - 1) / TZ};
-  const long long tiles_per = (long long)nt[0] * nt[1] * nt[2];
   double* t;
   uint8_t* code;
   double* kL;
@@ -290,11 +277,6 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     P.code = code + s * N;
     P.kL = kL + s * N;
     P.kd = kd + s * N;
-    P.nt[0] = nt[0];
-    P.nt[1] = nt[1];
-    P.nt[2] = nt[2];
-    P.tbase = s * tiles_per;
-    P.tinv = (double)QBUCKETS / m.tscale;
     {
       // about one node's traveltime at the largest velocity
       double dh[3];
@@ -311,20 +293,11 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   std::memset(&sa, 0, sizeof sa);
   sa.nprob = (int32_t)nsrc;
   sa.nd = g.nd;
-  sa.ntiles = tiles_per * nsrc;
-  // per-bucket ring capacity: the front occupies a small fraction of all tiles at a time
-  unsigned long long cap = 1;
-  const unsigned long long want = std::max<unsigned long long>((unsigned long long)sa.ntiles / 16, 1ull << 16);
-  while (cap < want) cap <<= 1;
-  sa.q.mask = cap - 1;
   unsigned long long* ctr;
-  GET(ctr, unsigned long long, "q_ctr", 2 * QBUCKETS + 8);
-  sa.q.head = ctr;
-  sa.q.tail = ctr + QBUCKETS;
-  sa.activations = ctr + 2 * QBUCKETS;
-  sa.node_evals = ctr + 2 * QBUCKETS + 1;
-  sa.pending = (int32_t*)(ctr + 2 * QBUCKETS + 2);
-  sa.abort_flag = (int32_t*)(ctr + 2 * QBUCKETS + 3);
+  GET(ctr, unsigned long long, "solve_ctr", 16);
+  sa.activations = ctr;
+  sa.node_evals = ctr + 1;
+  sa.abort_flag = (int32_t*)(ctr + 2);
   // round-solver state, shared by the refined windows' solve and the coarse solve
   const long long rsn = nsrc * std::max<long long>(N, refine ? fb.nfmax : 1);
   if ((unsigned long long)rsn >= (1ull << 32))
@@ -349,9 +322,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   sa.rs.stride = (unsigned long long)N;
   sa.err = fb.err;
   sa.probs = dp;
-  sa.max_activations = 400ull * (unsigned long long)sa.ntiles + 100000ull;
-  sa.max_passes = 4096;
-  sa.gate = 1.0;
+  sa.max_activations = ~0ull;
   sa.timeout_ns = 20LL * 1000 * 1000 * 1000;
   // refined windows: one more round-solver problem per source
   CoarseProblem* fprobs = nullptr;

@@ -12,7 +12,6 @@
 // the grid in traveltime order. Every wait is bounded (global timer), the number of rounds
 // is bounded; both report through an error word instead of trapping.
 #include "kernels.cuh"
-#include "queue.cuh"
 #include "rounds.cuh"
 
 namespace eik {
@@ -38,30 +37,6 @@ __global__ void coarse_init_kernel(const CoarseProblem* probs, int nprob, long l
   }
 }
 
-__global__ void queue_init_kernel(SolveArgs a) {
-  const long long cap = (long long)a.q.mask + 1;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < cap * QBUCKETS;
-       q += (long long)gridDim.x * blockDim.x)
-    a.q.seq[q] = (unsigned long long)(q % cap);
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < a.ntiles;
-       q += (long long)gridDim.x * blockDim.x) {
-    a.tile_faces[q] = 0;
-    a.tile_flag[q] = 0;
-    a.tile_prio[q] = (unsigned long long)__double_as_longlong(EIK_INF);
-  }
-  if (blockIdx.x == 0 && threadIdx.x < QBUCKETS) {
-    a.q.head[threadIdx.x] = 0;
-    a.q.tail[threadIdx.x] = 0;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *a.pending = 0;
-    *a.activations = 0;
-    *a.node_evals = 0;
-    *a.abort_flag = 0;
-  }
-}
-
-
 __global__ void rounds_init_kernel(SolveArgs a) {
   const long long tot = (long long)a.rs.stride * a.nprob;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot;
@@ -84,7 +59,6 @@ __global__ void rounds_init_kernel(SolveArgs a) {
     a.rs.bar[1] = 0;
     *a.rs.rounds = 0;
     for (int k = 0; k < 7; k++) a.rs.visits[k] = 0;
-    *a.pending = 0;
     *a.activations = 0;
     *a.node_evals = 0;
     *a.abort_flag = 0;
@@ -501,8 +475,6 @@ void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const doub
   if (sa.nd == 3) seed_kernel<3><<<sa.nprob, 128, 0, st>>>(sa, seed_lin, seed_tt, out, fine_corners ? 1 : 0, seedcap);
   else seed_kernel<2><<<sa.nprob, 128, 0, st>>>(sa, seed_lin, seed_tt, out, fine_corners ? 1 : 0, seedcap);
 }
-
-void launch_queue_init(const SolveArgs& sa, cudaStream_t st) { queue_init_kernel<<<296, 256, 0, st>>>(sa); }
 
 template <int ND>
 static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st) {

@@ -504,10 +504,6 @@ __global__ void fine_setup_kernel(ForwardBatch fb, CoarseProblem* fprobs, double
   P.code = fb.fine_code + (size_t)s * fb.nfmax;
   P.kL = fkL + (size_t)s * fb.nfmax;
   P.kd = fkd + (size_t)s * fb.nfmax;
-  for (int d = 0; d < 3; d++) P.nt[d] = 1;
-  P.pad = 0;
-  P.tbase = 0;
-  P.tinv = 1.0;
   double dh[3];
   node_dh(gf, 0, dh);
   double hmin = dh[0];

@@ -60,25 +60,8 @@ struct CoarseProblem {
   uint8_t* code;   // packed derivative codes; bit 7: special key (source or non-causal)
   double* kL;      // key level of special nodes (-inf for source points)
   uint8_t* kd;     // key depth of special nodes
-  int32_t nt[3];   // tiles per axis
-  int32_t pad;
-  long long tbase; // first global tile id of this problem
-  double tinv;     // QBUCKETS / (time scale of this problem): trigger time -> bucket
   double delta;    // round width of the forward solve (traveltime units)
   double incmin;   // smallest increment of the local update over a neighbour: (2/3) h s_min / sqrt(nd)
-};
-
-// Bucketed priority queue of tile ids: QBUCKETS bounded multi-producer/multi-consumer
-// rings (Vyukov's sequence scheme), bucket = trigger time of the tile scaled by its
-// problem's time scale. Consumers take from the lowest non-empty bucket, so tiles are
-// processed roughly in the order the fast-marching front reaches them.
-constexpr int QBUCKETS = 64;
-struct TileQueue {
-  unsigned long long* items;  // QBUCKETS x (mask+1)
-  unsigned long long* seq;    // QBUCKETS x (mask+1)
-  unsigned long long* head;   // QBUCKETS
-  unsigned long long* tail;   // QBUCKETS
-  unsigned long long mask;
 };
 
 // Worklists and thresholds of the round-synchronous forward solve. Nodes are numbered
@@ -103,24 +86,15 @@ struct SolveArgs {
   const CoarseProblem* probs;
   int32_t nprob;
   int32_t nd;
-  long long ntiles;            // total tiles over all problems
-  uint32_t* tile_faces;        // pending dirty faces per tile (bit 6: whole tile)
-  unsigned long long* tile_prio;  // smallest pending trigger time per tile (double bits)
-  int32_t* tile_flag;          // 1 while queued
-  TileQueue q;
-  int32_t* pending;            // tiles queued or being processed
-  unsigned long long* activations;
+  unsigned long long* activations;  // list entries visited
   unsigned long long max_activations;
   unsigned long long* node_evals;
   uint32_t* err;
   int32_t* abort_flag;
-  int32_t max_passes;
-  double gate;                 // in-tile front gate, in units of (node spacing x slowness)
   long long timeout_ns;
   RoundState rs;
 };
 
-constexpr uint32_t FACES_ALL = 1u << 6;
 
 // launchers (defined in the .cu files)
 void launch_srcbox(const ForwardBatch& fb, cudaStream_t st);
@@ -141,7 +115,6 @@ void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, double smi
 void launch_fine_select(const ForwardBatch& fb, const CoarseProblem* fprobs, uint8_t* fine_tie, cudaStream_t st);
 void launch_fine_replay(const ForwardBatch& fb, const int32_t* srclist, int n, cudaStream_t st);
 cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
-void launch_queue_init(const SolveArgs& sa, cudaStream_t st);  // empty queue, idle tiles, zero counters
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);
 

@@ -3,9 +3,20 @@
 #pragma once
 
 #include "kernels.cuh"
-#include "queue.cuh"
 
 namespace eik {
+
+constexpr int SOLVE_THREADS = 256;  // threads per CTA of the round kernels
+
+__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long* p) {
+  return *(volatile const unsigned long long*)p;
+}
+
+__device__ __forceinline__ long long gtimer_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // Grid-wide barrier of the cooperative solve launch (all CTAs co-resident). The wait is
 // bounded by the global timer; a CTA that gives up raises the abort flag, which releases

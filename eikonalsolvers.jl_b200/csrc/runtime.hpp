@@ -38,7 +38,6 @@ struct Model {
   long long N = 0;
   double* vel = nullptr;   // device
   double* slow = nullptr;  // device, 1.0/vel
-  double tscale = 1.0;     // grid diagonal x mean slowness (tile scheduling only)
   double smin = 0.0;       // smallest slowness of the model (round width of the forward solve)
 };
 

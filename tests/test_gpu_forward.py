@@ -96,3 +96,22 @@ def test_asserts_mirror_reference(ctx):
     out[0, 0] = -1.0
     with pytest.raises(AssertionError):
         _run(ctx, c["vel"], c["grd"], out, c["coordrec"], c["extraparams"])
+
+
+@pytest.mark.parametrize("which", ["3Dconst1", "3Dlingrad3", "2Dconst3", "cfg3"])
+def test_refined_startup_fixed_point_equals_heap_replay(ctx, which):
+    """The refined window solved as a fixed point with its stop reconstructed from keys gives
+    the same traveltimes as the exact heap replay (sources with a tied stop are replayed)."""
+    if which == "cfg3":
+        w = CF.cfg3(scale=0.25, nsrc=6, nrec_side=5)
+        vel, grd, cs, rec, ep = w.vel, w.grd, w.coordsrc, w.coordrec, ExtraParams()
+    else:
+        c = [c for c in RC.all_forward_cases() if c["name"] == which][0]
+        vel, grd, cs, rec, ep = c["vel"], c["grd"], c["coordsrc"], c["coordrec"], c["extraparams"]
+    out = []
+    for mode in (1, 0):
+        ctx.set_param("fine_replay", mode)
+        out.append(_run(ctx, vel, grd, cs, rec, ep))
+    ctx.set_param("fine_replay", 0)
+    for a, b in zip(out[0][1], out[1][1]):
+        assert np.array_equal(a, b)
