@@ -103,7 +103,7 @@ __global__ void adj_prep_kernel(const CoarseProblem* probs, const AdjProblem* ap
     sa.rs.stamp[q] = ndep;
     if (ndep == 0 && !src) {
       const unsigned int at = atomicAdd(sa.rs.cnt, 1u);
-      sa.rs.list[0][at] = (unsigned int)q;
+      sa.rs.list[0][at] = (unsigned long long)q << 32;
     }
   }
 }
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) adj_rounds_kernel(AdjArgs aa) {
     const int b3 = r % 3;
     const unsigned int n = *(volatile unsigned int*)(a.rs.cnt + b3);
     if (n == 0) break;
-    const unsigned int* L = a.rs.list[r & 1];
+    const unsigned long long* L = a.rs.list[r & 1];
     for (;;) {
       unsigned int base = 0;
       if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) adj_rounds_kernel(AdjArgs aa) {
       const unsigned int idx = base + lane;
       unsigned int rel[6] = {~0u, ~0u, ~0u, ~0u, ~0u, ~0u};
       if (idx < n) {
-        const unsigned int gid = L[idx];
+        const unsigned int gid = (unsigned int)(L[idx] >> 32);
         const int prob = (int)(gid / N);
         const unsigned long long gb = (unsigned long long)prob * N;
         adj_node<ND>(aa, prob, (long long)(gid - gb), gb, rel);

@@ -305,8 +305,8 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   GET(sa.rs.stamp, int32_t, "rs_stamp", rsn);
   GET(sa.rs.tent, double, "rs_tent", rsn);
   GET(sa.rs.dirty, uint8_t, "rs_dirty", rsn);
-  GET(sa.rs.list[0], unsigned int, "rs_list0", rsn);
-  GET(sa.rs.list[1], unsigned int, "rs_list1", rsn);
+  GET(sa.rs.list[0], unsigned long long, "rs_list0", rsn);
+  GET(sa.rs.list[1], unsigned long long, "rs_list1", rsn);
   GET(sa.rs.nextmin, unsigned long long, "rs_nextmin", 3 * nsrc);
   GET(sa.rs.thr, double, "rs_thr", 2 * nsrc);
   {

@@ -17,11 +17,18 @@
 namespace eik {
 
 
-// Lists node gid (problem * N + node) for round r, once per round.
-__device__ __forceinline__ void list_node(const SolveArgs& a, int r, unsigned int gid) {
+// Worklist entry: node id (problem * N + node) in the high word, a lower bound of the
+// node's pending front (float, rounded down) in the low word.
+__device__ __forceinline__ unsigned long long list_entry(unsigned int gid, double front) {
+  const float f = front < EIK_INF ? __double2float_rd(front) : __int_as_float(0x7f800000);
+  return ((unsigned long long)gid << 32) | (unsigned long long)__float_as_uint(f);
+}
+
+// Lists node gid for round r, once per round.
+__device__ __forceinline__ void list_node(const SolveArgs& a, int r, unsigned int gid, double front) {
   if (atomicExch(a.rs.stamp + gid, r) != r) {
     const unsigned int i = atomicAdd(a.rs.cnt + (r % 3), 1u);
-    a.rs.list[r & 1][i] = gid;
+    a.rs.list[r & 1][i] = list_entry(gid, front);
   }
 }
 
@@ -98,11 +105,27 @@ __global__ void seed_kernel(SolveArgs a, const int32_t* seed_lin, const double* 
         int p[3] = {c[0], c[1], c[2]};
         p[ax] += d;
         if (p[ax] < 0 || p[ax] >= P.g.n[ax]) continue;
-        list_node(a, 0, (unsigned int)(gbase + lin3(P.g, p[0], p[1], p[2])));
+        list_node(a, 0, (unsigned int)(gbase + lin3(P.g, p[0], p[1], p[2])), tt);
       }
   }
 }
 
+#ifdef EIK_PHASE
+// tuning builds only: clock cycles per phase summed over warps (lane 0)
+__device__ unsigned long long eik_phase[9];
+extern "C" int eik_phase_read(unsigned long long* out) {
+  return (int)cudaMemcpyFromSymbol(out, eik_phase, sizeof(unsigned long long) * 9);
+}
+#define PH_T(v) const long long v = clock64()
+#define PH_ADD(k, t0) if ((threadIdx.x & 31) == 0) atomicAdd(&eik_phase[k], (unsigned long long)(clock64() - (t0)))
+#define PL_T(v) const long long v = clock64()
+#define PL_ADD(k, t0) vk[k] += (unsigned long long)(clock64() - (t0))
+#else
+#define PH_T(v)
+#define PH_ADD(k, t0)
+#define PL_T(v)
+#define PL_ADD(k, t0)
+#endif
 // ------------------------------------------------------------------ node solve --
 // Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise.
 __device__ __forceinline__ void node_key(const CoarseProblem& P, long long l, double t, uint8_t cb, double* L, int* d) {
@@ -138,12 +161,13 @@ template <int ND>
 __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, unsigned long long gbase, long long l,
                                  double T, int r, double* front, unsigned long long* evals,
                                  unsigned long long* vk) {
+  PL_T(tq0);
   const GridDesc& g = P.g;
   const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
   // last evaluated value, still valid while nothing the node reads has changed
   if (!__ldcg(a.rs.dirty + gbase + l)) {
     const double tv = __ldcg(a.rs.tent + gbase + l);
-    if (tv > T) {
+    if (tv > T && tv < EIK_INF) {
       *front = tv;
       vk[0]++;
       return 1u << DIR_SELF;
@@ -158,6 +182,10 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     vk[1]++;
     return 0;
   }
+  // from here the node reads its neighbours' current values: a change after this point
+  // marks it dirty again (writers store the value, fence, then the flag)
+  a.rs.dirty[gbase + l] = 0;
+  __threadfence();
   // immediate neighbours: potential (the smallest of their traveltimes)
   double t1[ND][2];
   long long l1[ND][2];
@@ -177,9 +205,12 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
       pot = fmin(pot, t1[ax][s]);
     }
   if (!(pot < EIK_INF)) {  // nothing reached around it yet
+    a.rs.tent[gbase + l] = EIK_INF;
     vk[2]++;
     return 0;
   }
+  PL_ADD(7, tq0);
+  PL_T(tq1);
   Nbhd nb;
   nb_clear(nb);
   node_dh(g, c[0], nb.dh);
@@ -192,14 +223,11 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   for (int ax = 1; ax < ND; ax++) hmin = fmin(hmin, nb.dh[ax]);
   const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * nb.slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
   if (lb > T) {
+    a.rs.tent[gbase + l] = lb;  // stands, like an evaluated value, while the node stays clean
     *front = lb;
     vk[3]++;
     return 1u << DIR_SELF;
   }
-  // from here the node is evaluated with the neighbours' current values: a change after
-  // this point marks it dirty again (writers store the value, fence, then the flag)
-  a.rs.dirty[gbase + l] = 0;
-  __threadfence();
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
@@ -227,7 +255,9 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   int8_t cd[3] = {0, 0, 0};
   Key nk;
   bool neg = false;
+  PL_T(tq2);
   const double nv = prefix_rule<ND>(nb, cd, &nk, &neg);
+  PL_ADD(9, tq2);
   (*evals)++;
   const uint8_t nc = pack_codes(cd, ND);
   const bool same_t = (nv == told) || (isinf(nv) && isinf(told));
@@ -252,6 +282,7 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     P.kd[l] = (uint8_t)nk.d;
   }
   __threadfence();
+  PL_T(tq3);
   // The nodes whose stencil reads this one (+-1, +-2 along each axis) are evaluated again,
   // except those whose stored key is at most both the old and the new key of this node:
   // the order rule of such a node never accepts this one, nor is its termination test
@@ -285,6 +316,8 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     dirs |= 1u << k;
   }
   *front = nv + P.incmin;  // no node reading this one can get a smaller value from it
+  PL_ADD(10, tq3);
+  PL_ADD(8, tq1);
   vk[6]++;
   return dirs;
 }
@@ -304,15 +337,19 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
   const int lane = threadIdx.x & 31;
   const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
   unsigned long long evals = 0;
+#ifdef EIK_PHASE
+  unsigned long long vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles: gates, node path, rule, relist filter
+#else
   unsigned long long vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
+#endif
   int r = 0;
   for (; r < a.rs.max_rounds; r++) {
     const int b3 = r % 3, nb3 = (r + 1) % 3;
     const unsigned int n = *(volatile unsigned int*)(a.rs.cnt + b3);
     if (n == 0) break;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.activations, (unsigned long long)n);  // list entries
-    const unsigned int* L = a.rs.list[r & 1];
-    unsigned int* Lnext = a.rs.list[(r + 1) & 1];
+    const unsigned long long* L = a.rs.list[r & 1];
+    unsigned long long* Lnext = a.rs.list[(r + 1) & 1];
     const unsigned long long* nm = a.rs.nextmin + (size_t)b3 * a.nprob;
     unsigned long long* nmn = a.rs.nextmin + (size_t)nb3 * a.nprob;
     const double* thr_prev = a.rs.thr + (size_t)((r + 1) & 1) * a.nprob;  // thresholds of round r-1
@@ -321,26 +358,41 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
       for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
         thr_cur[p] = fmax(thr_prev[p], __longlong_as_double((long long)ld_volatile(nm + p)) + a.probs[p].delta);
     for (;;) {
+      PH_T(tg);
       unsigned int base = 0;
       if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
       base = __shfl_sync(0xffffffffu, base, 0);
+      PH_ADD(0, tg);
       if (base >= n) break;
+      PH_T(tp);
       const unsigned int idx = base + lane;
       unsigned dirs = 0;
       double front = EIK_INF;
       int prob = 0;
       long long l = 0;
       if (idx < n) {
-        const unsigned int gid = L[idx];
+        const unsigned long long e = L[idx];
+        const unsigned int gid = (unsigned int)(e >> 32);
+        const double ef = (double)__uint_as_float((unsigned int)e);
         prob = (int)(gid / N);
         l = (long long)(gid - (unsigned long long)prob * N);
         const CoarseProblem& P = a.probs[prob];
         // window of one round width above the smallest pending front, never moving back
         const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
         const unsigned long long gb = (unsigned long long)prob * N;
-        dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
-                         : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
+        if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
+          // still waiting and nothing it reads has changed: its front stands
+          front = ef;
+          dirs = 1u << DIR_SELF;
+          vk[0]++;
+        } else {
+          dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
+                           : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
+        }
       }
+      __syncwarp();
+      PH_ADD(1, tp);
+      PH_T(ts);
       // list the next round's nodes once each (per-node round stamps)
       const CoarseProblem& P = a.probs[prob];
       const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
@@ -357,6 +409,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
         }
         if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
       }
+      __syncwarp();
+      PH_ADD(2, ts);
+      PH_T(ta);
       // warp-aggregated append: one atomic per 32 nodes
       const int cntl = __popc(keep);
       int incl = cntl;
@@ -377,9 +432,21 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
           p[k >> 2] += dir_off(k);
           nl = lin3(P.g, p[0], p[1], p[2]);
         }
-        Lnext[wbase++] = (unsigned int)(gbase + nl);
+        Lnext[wbase++] = list_entry((unsigned int)(gbase + nl), front);
       }
-      if (keep) atomic_min_pos(nmn + prob, front);
+      {
+        // one update per problem and warp: the lanes of a problem agree on their smallest front
+        const double fv = keep ? front : EIK_INF;
+        const unsigned grp = __match_any_sync(0xffffffffu, prob);
+        double gmin = fv;
+        for (unsigned m = grp; m; m &= m - 1) {
+          const int src = __ffs(m) - 1;
+          gmin = fmin(gmin, __shfl_sync(grp, fv, src));
+        }
+        if (lane == __ffs(grp) - 1) atomic_min_pos(nmn + prob, gmin);
+      }
+      __syncwarp();
+      PH_ADD(3, ta);
     }
     // buffers of round r+2 (last used in round r-1)
     if (blockIdx.x == 0) {
@@ -391,11 +458,16 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
       for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
         a.rs.nextmin[(size_t)c3 * a.nprob + p] = (unsigned long long)__double_as_longlong(EIK_INF);
     }
+    PH_T(tb);
     if (!grid_barrier(a)) break;
+    PH_ADD(4, tb);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
   if (lane == 0 && evals) atomicAdd(a.node_evals, evals);
+#ifdef EIK_PHASE
+  for (int k = 7; k < 11; k++) atomicAdd(&eik_phase[k - 2], vk[k]);  // per lane
+#endif
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     unsigned long long v = vk[k];
@@ -478,14 +550,15 @@ void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const doub
 
 template <int ND>
 static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st) {
+  const size_t sm = 0;
   int per = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND>, SOLVE_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND>, SOLVE_THREADS, sm);
   per = per < 1 ? 1 : per;
   SolveArgs args = sa;
   void* kargs[] = {&args};
   // cooperative: every CTA is resident, so the grid barrier between rounds cannot deadlock
   return cudaLaunchCooperativeKernel((const void*)coarse_rounds_kernel<ND>, dim3(nsm * per), dim3(SOLVE_THREADS),
-                                     kargs, 0, st);
+                                     kargs, sm, st);
 }
 
 cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st) {

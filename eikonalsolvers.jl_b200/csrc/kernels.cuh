@@ -70,7 +70,7 @@ struct RoundState {
   int32_t* stamp;               // per node: last round it was listed for
   double* tent;                 // per node: value of its last evaluation
   uint8_t* dirty;               // per node: something it reads changed since that evaluation
-  unsigned int* list[2];        // node ids of the current and the next round
+  unsigned long long* list[2];  // entries of the current and the next round (node id << 32 | front)
   unsigned int* cnt;            // [3] list length per round (mod 3)
   unsigned int* grab;           // [3] next list entry to take per round (mod 3)
   unsigned long long* nextmin;  // [3][nprob] smallest pending potential (double bits)

@@ -66,7 +66,7 @@ __device__ __forceinline__ void warp_append(const SolveArgs& a, int r, bool have
   unsigned int base = 0;
   if (lane == 0) base = atomicAdd(a.rs.cnt + (r % 3), (unsigned int)__popc(m));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (have) a.rs.list[r & 1][base + __popc(m & ((1u << lane) - 1u))] = val;
+  if (have) a.rs.list[r & 1][base + __popc(m & ((1u << lane) - 1u))] = (unsigned long long)val << 32;
 }
 
 }  // namespace eik
