@@ -87,12 +87,13 @@ def measured_peaks():
 
 
 def profile_traffic(name):
-    """DRAM bytes per launch of a kernel from a committed ncu summary, if one exists:
-    a line `traffic_bytes_per_source_solve: <float>` in profiles/<name>.md."""
+    """DRAM bytes per node-solve of a kernel from a committed ncu summary, if one exists:
+    a line `traffic_bytes_per_node_solve: <float>` in profiles/<name>.md (captured on a
+    smaller case; traffic grows with the node-solves of a launch)."""
     p = os.path.join(REPO, "profiles", name + ".md")
     if not os.path.exists(p):
         return None
-    m = re.search(r"traffic_bytes_per_source_solve:\s*([0-9.eE+]+)", open(p).read())
+    m = re.search(r"traffic_bytes_per_node_solve:\s*([0-9.eE+]+)", open(p).read())
     return float(m.group(1)) if m else None
 
 
@@ -382,7 +383,8 @@ def main_b200(args):
     traffic_ss = profile_traffic(top)
     roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
-            "traffic": (traffic_ss * nsrc if traffic_ss is not None else None),
+            "traffic": (traffic_ss * N * nsrc if traffic_ss is not None else None),
+            "traffic_note": "DRAM bytes per launch scaled from the per-node-solve figure of profiles/<kernel>.md",
             "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms,
             "share_of_step": kms / ms,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()}}
