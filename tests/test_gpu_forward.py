@@ -115,3 +115,15 @@ def test_refined_startup_fixed_point_equals_heap_replay(ctx, which):
     ctx.set_param("fine_replay", 0)
     for a, b in zip(out[0][1], out[1][1]):
         assert np.array_equal(a, b)
+
+
+def test_many_sources_batched_at_128cubed_match_the_oracle(ctx):
+    """16 sources of the 3D layered workload at 128^3 in one call (many sources in flight in
+    every round): the sources checked are bit-identical to the oracle's FMM."""
+    w = CF.cfg3(scale=0.5, nsrc=16, nrec_side=5)
+    picks, tt = _run(ctx, w.vel, w.grd, w.coordsrc, w.coordrec, ExtraParams())
+    for s in (0, 7, 15):
+        op, ott = O.eiktraveltime(w.vel, w.grd, w.coordsrc[s:s + 1], w.coordrec[s:s + 1], returntt=True,
+                                  extraparams=ExtraParams())
+        assert int((tt[s] != ott[0]).sum()) == 0, s
+        assert np.array_equal(picks[s], op[0])
