@@ -944,8 +944,6 @@ static int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t
     return fail(ctx, EIK_ERR_ASSERT, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)");
   int rc = check_extra(ctx, &ep);
   if (rc) return rc;
-  if (ep.smoothgradkern > 0)
-    return fail(ctx, EIK_ERR_UNSUPPORTED, "smoothgradkern>0 (Gaussian smoothing of the summed gradient) is not built");
   if (nsrc <= 0) return fail(ctx, EIK_ERR_ASSERT, "nsrc >= 1");
   if ((whichgrad == 2 || whichgrad == 3) && !is_cart(m.g))
     return fail(ctx, EIK_ERR_ERROR, "type %s has no field hgrid", m.g.nd == 2 ? "Grid2DSphere" : "Grid3DSphere");
@@ -977,7 +975,7 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   if (!var) return rc == EIK_ERR_OUT_OF_BUDGET                                       \
                      ? fail(ctx, rc, "scratch '%s' exceeds the HBM budget", name)    \
                      : fail(ctx, rc, "cudaMalloc of scratch '%s' failed", name);
-  double *lam, *gdt, *rhs, *misf, *dpsi, *ysrc, *gnode, *gsrc, *flam, *fgdt, *carry;
+  double *lam, *gdt, *rhs, *misf, *dpsi, *ysrc, *gnode, *gsrc, *flam, *fgdt, *carry, *gsum, *gw;
   AdjProblem* dap;
   ForwardBatch* dfb;
   uint32_t* dwarn;
@@ -992,6 +990,13 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   GET(gsrc, double, "adj_gsrc", nsrc * nd);
   GET(flam, double, "adj_fine_lam", ep.refinearoundsrc ? nsrc * fw.fb.nfmax : 1);
   GET(fgdt, double, "adj_fine_gdt", ep.refinearoundsrc ? nsrc * nd * fw.fb.nfmax : 1);
+  // smoothgradkern > 0: the group sum goes to a scratch field, the smoothing writes the output
+  const bool smoothing = wantvel && d_gradvel && ep.smoothgradkern > 0;
+  const long long nker = smoothing ? (nd == 3 ? (long long)ep.smoothgradkern * ep.smoothgradkern * ep.smoothgradkern
+                                              : (long long)ep.smoothgradkern * ep.smoothgradkern)
+                                   : 1;
+  GET(gsum, double, "adj_gradsum", smoothing ? N : 1);
+  GET(gw, double, "adj_smooth_w", nker);
   GET(dap, AdjProblem, "adj_probs", nsrc);
   GET(dfb, ForwardBatch, "adj_fb", 1);
   GET(dwarn, uint32_t, "adj_warn", 1);
@@ -1058,7 +1063,13 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
     adj_carry_kernel<<<(int)nsrc, 64, 0, st>>>(ta, ep.radiussmoothgradsrc, carry);
     adj_srcnodes_kernel<<<(int)nsrc, 128, 0, st>>>(ta, carry);
     if (ep.radiussmoothgradsrc > 0) adj_smooth_kernel<<<(int)nsrc, 256, 0, st>>>(ta, ep.radiussmoothgradsrc);
-    if (d_gradvel) adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ngroups, N, d_gradvel);
+    if (d_gradvel) adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ngroups, N, smoothing ? gsum : d_gradvel);
+    if (smoothing) {
+      // weights from pageable memory: the copy has left the vector when cudaMemcpyAsync returns
+      const std::vector<double> w = gaussian_weights((int)ep.smoothgradkern, nd);
+      CUDA_OK(ctx, cudaMemcpyAsync(gw, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, st));
+      CUDA_OK(ctx, launch_smoothgrad(m.g, (int)ep.smoothgradkern, gw, gsum, d_gradvel, st));
+    }
   }
   if (d_misfit) adj_misfit_kernel<<<1, 1, 0, st>>>(misf, (int)nsrc, ngroups, d_misfit);
   if (d_gradsrc && whichgrad != 1)
@@ -1073,7 +1084,8 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
     stats->warn_mask |= hw;
     stats->adj_rounds = (uint64_t)arounds;
     stats->launches += 7 + (d_misfit ? 1 : 0) +
-                       (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0);
+                       (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0) +
+                       (smoothing ? 1 : 0);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->evk[4], ctx->evk[5]);
     stats->adj_ms = ms;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "common.cuh"
 
@@ -117,5 +118,10 @@ void launch_fine_replay(const ForwardBatch& fb, const int32_t* srclist, int n, c
 cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);
+// Gaussian smoothing of a gradient field (smoothgradkern = l, odd): weights on the host,
+// then one launch from in to out (distinct buffers); d_w holds gaussian_weights(l, nd).
+std::vector<double> gaussian_weights(int l, int dim);
+cudaError_t launch_smoothgrad(const GridDesc& g, int l, const double* d_w, const double* in, double* out,
+                              cudaStream_t st);
 
 }  // namespace eik

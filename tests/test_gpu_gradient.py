@@ -181,3 +181,23 @@ def test_gradsrcloc_fd_on_gpu(ctx):
         ctx.release(mid)
     d = np.abs(gs - fd)
     assert d.max() <= 1.015 * case["tolerr"] and np.linalg.norm(d) <= 1.015 * case["tolnorm"], (gs, fd)
+
+
+@pytest.mark.parametrize("kind,l", [("2D", 5), ("3D", 3), ("3D", 23)])
+def test_smoothgradkern(ctx, kind, l):
+    """ExtraParams.smoothgradkern = l: the summed gradient is smoothed on the device. The
+    smoothed GPU gradient is bit-identical to the oracle's smoothgradient applied to the
+    GPU's unsmoothed gradient (same weights, same summation order; 3D with l = 23 takes the
+    unstaged kernel), and within the gradient tolerance of the oracle's eikgradient."""
+    if kind == "2D":
+        w = CF.cfg2(scale=0.125, nsrc=3, forward=lambda v, g, c, r, e: O.eiktraveltime(v, g, c, r, extraparams=e))
+    else:
+        w = CF.cfg3(scale=0.125, nsrc=2, nrec_side=5,
+                    forward=lambda v, g, c, r, e: O.eiktraveltime(v, g, c, r, extraparams=e))
+    ep = ExtraParams(smoothgradkern=l)
+    g, m = _gpu_grad(ctx, w.vel, w.grd, w.coordsrc, w.coordrec, w.pickobs, w.stdobs, "gradvel", ep)
+    g0, m0 = _gpu_grad(ctx, w.vel, w.grd, w.coordsrc, w.coordrec, w.pickobs, w.stdobs, "gradvel", ExtraParams())
+    assert m == m0
+    assert np.array_equal(g, O.smoothgradient(l, w.grd, g0))
+    o = O.eikgradient(w.vel, w.grd, w.coordsrc, w.coordrec, w.pickobs, w.stdobs, "gradvel", extraparams=ep)
+    _check((g, m), o, "gradvel")
