@@ -939,7 +939,7 @@ __global__ void adj_misfit_kernel(const double* misf, int nsrc, int nw, double* 
 
 namespace eik {
 
-static int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichgrad, const eik_extra& ep) {
+int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichgrad, const eik_extra& ep) {
   if (whichgrad < 1 || whichgrad > 3)
     return fail(ctx, EIK_ERR_ASSERT, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)");
   int rc = check_extra(ctx, &ep);
@@ -955,10 +955,10 @@ static int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t
 // Forward + adjoint + assembly for nsrc sources whose inputs are on the device.
 // Outputs (each nullable): d_gradvel N values, d_gradsrc nsrc x nd, d_misfit 1 value.
 // Returns after the stream has drained and the device error word has been checked.
-static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
+int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
                          const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
                          const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit,
-                         eik_stats* stats) {
+                         eik_stats* stats, GradTail* tail_out) {
   int rc = EIK_OK;
   cudaStream_t st = ctx->stream;
   Scratch& S = ctx->scratch;
@@ -1007,8 +1007,11 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
     hap[s].gdt = gdt + s * N * nd;
     hap[s].rhs = rhs + s * N;
   }
-  CUDA_OK(ctx, cudaMemcpyAsync(dap, hap.data(), sizeof(AdjProblem) * nsrc, cudaMemcpyHostToDevice, st));
-  CUDA_OK(ctx, cudaMemcpyAsync(dfb, &fw.fb, sizeof(ForwardBatch), cudaMemcpyHostToDevice, st));
+  const void* hap_src = stage_host(ctx, hap.data(), sizeof(AdjProblem) * nsrc);
+  const void* fb_src = stage_host(ctx, &fw.fb, sizeof(ForwardBatch));
+  if (!hap_src || !fb_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
+  CUDA_OK(ctx, cudaMemcpyAsync(dap, hap_src, sizeof(AdjProblem) * nsrc, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(dfb, fb_src, sizeof(ForwardBatch), cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemsetAsync(dwarn, 0, sizeof(uint32_t), st));
   CUDA_OK(ctx, cudaMemsetAsync(gsrc, 0, sizeof(double) * nsrc * nd, st));
   const CoarseProblem* dprobs = fw.sa.probs;
@@ -1033,9 +1036,9 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   ra.misfit = misf;
   ra.dpsi = dpsi;
   adj_recv_kernel<<<(int)((nsrc + 63) / 64), 64, 0, st>>>(ra);
-  cudaEventRecord(ctx->evk[4], st);
+  if (!ctx->capturing) cudaEventRecord(ctx->evk[4], st);
   CUDA_OK(ctx, nd == 3 ? launch_adj_solve<3>(aa, ctx->solve_sms(), st) : launch_adj_solve<2>(aa, ctx->solve_sms(), st));
-  cudaEventRecord(ctx->evk[5], st);
+  if (!ctx->capturing) cudaEventRecord(ctx->evk[5], st);
   adj_check_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, N, fw.fb.err);
   CUDA_OK(ctx, cudaGetLastError());
   SrcTermArgs ta;
@@ -1067,7 +1070,9 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
     if (smoothing) {
       // weights from pageable memory: the copy has left the vector when cudaMemcpyAsync returns
       const std::vector<double> w = gaussian_weights((int)ep.smoothgradkern, nd);
-      CUDA_OK(ctx, cudaMemcpyAsync(gw, w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, st));
+      const void* w_src = stage_host(ctx, w.data(), sizeof(double) * w.size());
+      if (!w_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
+      CUDA_OK(ctx, cudaMemcpyAsync(gw, w_src, sizeof(double) * w.size(), cudaMemcpyHostToDevice, st));
       CUDA_OK(ctx, launch_smoothgrad(m.g, (int)ep.smoothgradkern, gw, gsum, d_gradvel, st));
     }
   }
@@ -1075,20 +1080,37 @@ static int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const doubl
   if (d_gradsrc && whichgrad != 1)
     CUDA_OK(ctx, cudaMemcpyAsync(d_gradsrc, gsrc, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToDevice, st));
   CUDA_OK(ctx, cudaGetLastError());
-  uint32_t hw = 0;
-  int32_t arounds = 0;
-  CUDA_OK(ctx, cudaMemcpyAsync(&hw, dwarn, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-  CUDA_OK(ctx, cudaMemcpyAsync(&arounds, aa.sa.rs.rounds, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-  rc = collect_forward_stats(ctx, &fw, stats);
+  GradTail tail;
+  tail.fw = fw;
+  tail.dwarn = dwarn;
+  tail.arounds = aa.sa.rs.rounds;
+  tail.launches = 7 + (d_misfit ? 1 : 0) +
+                  (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0) + (smoothing ? 1 : 0);
+  if (tail_out) *tail_out = tail;
+  if (ctx->capturing) return EIK_OK;  // read back after each replay of the captured graph
+  rc = gradient_tail_stats(ctx, tail, stats);
   if (stats) {
-    stats->warn_mask |= hw;
-    stats->adj_rounds = (uint64_t)arounds;
-    stats->launches += 7 + (d_misfit ? 1 : 0) +
-                       (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0) +
-                       (smoothing ? 1 : 0);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->evk[4], ctx->evk[5]);
     stats->adj_ms = ms;
+  }
+  return rc;
+}
+
+}  // namespace eik
+
+namespace eik {
+
+int gradient_tail_stats(eik_ctx* ctx, GradTail& tail, eik_stats* stats) {
+  uint32_t hw = 0;
+  int32_t arounds = 0;
+  CUDA_OK(ctx, cudaMemcpyAsync(&hw, tail.dwarn, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_OK(ctx, cudaMemcpyAsync(&arounds, tail.arounds, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  const int rc = collect_forward_stats(ctx, &tail.fw, stats);
+  if (stats) {
+    stats->warn_mask |= hw;
+    stats->adj_rounds = (uint64_t)arounds;
+    stats->launches += tail.launches;
   }
   return rc;
 }
@@ -1144,7 +1166,7 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
   }
   const bool wantvel = whichgrad == 1 || whichgrad == 3, wantsrc = whichgrad != 1;
   rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
-                     wantsrc ? d_gs : nullptr, d_m, stats);
+                     wantsrc ? d_gs : nullptr, d_m, stats, nullptr);
   if (rc) return rc;
   double hm = 0.0;
   CUDA_OK(ctx, cudaMemcpyAsync(&hm, d_m, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1197,7 +1219,7 @@ extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsr
   CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
   rc = gradient_core(ctx, m, nsrc, coordsrc_dev, d_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad, ep,
                      (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
-                     misfit_dev, stats);
+                     misfit_dev, stats, nullptr);
   if (rc) return rc;
   cudaEventRecord(ctx->ev1, st);
   CUDA_OK(ctx, cudaStreamSynchronize(st));

@@ -157,6 +157,33 @@ __global__ void slowness_kernel(const double* vel, double* slow, long long n, in
   atomicMin(smin, (unsigned long long)__double_as_longlong(mn));  // positive doubles order as integers
 }
 
+void model_refresh(const Model& m, cudaStream_t st) {
+  cudaMemsetAsync(m.dstat, 0, 2 * sizeof(double), st);
+  cudaMemsetAsync(m.dstat + 2, 0x7f, sizeof(double), st);  // a large positive double
+  slowness_kernel<<<592, 256, 0, st>>>(m.vel, m.slow, m.N, reinterpret_cast<int*>(m.dstat), m.dstat + 1,
+                                       reinterpret_cast<unsigned long long*>(m.dstat + 2));
+}
+
+const void* stage_host(eik_ctx* ctx, const void* src, size_t bytes) {
+  if (!ctx->capturing || bytes == 0) return src;
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+  std::memcpy(p, src, bytes);
+  ctx->stage_arena->push_back(p);
+  return p;
+}
+
+// Round width and lower-bound increment of every coarse problem from the model's smallest
+// slowness, read on the device (the expressions and their order are the host's).
+__global__ void problem_scale_kernel(CoarseProblem* dp, int nprob, const double* dsmin, double gate, double hmin,
+                                     int nd) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nprob) return;
+  const double smin = *dsmin;
+  dp[s].delta = gate * hmin * smin;
+  dp[s].incmin = 0.999 * (2.0 / 3.0) * hmin * smin / sqrt((double)nd);
+}
+
 int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev, eik_model_id* out) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   Model m;
@@ -171,23 +198,16 @@ int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev,
   CUDA_OK(ctx, cudaMalloc(&m.slow, bytes));
   if (dev) CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
   else CUDA_OK(ctx, cudaMemcpyAsync(m.vel, vel, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  int* dflag = nullptr;
-  CUDA_OK(ctx, cudaMalloc(&dflag, 3 * sizeof(double)));
-  CUDA_OK(ctx, cudaMemsetAsync(dflag, 0, 2 * sizeof(double), ctx->stream));
-  CUDA_OK(ctx, cudaMemsetAsync(reinterpret_cast<double*>(dflag) + 2, 0x7f, sizeof(double), ctx->stream));
-  double* dsum = reinterpret_cast<double*>(dflag) + 1;
-  unsigned long long* dmin = reinterpret_cast<unsigned long long*>(dflag) + 2;
-  slowness_kernel<<<592, 256, 0, ctx->stream>>>(m.vel, m.slow, m.N, dflag, dsum, dmin);
+  CUDA_OK(ctx, cudaMalloc(&m.dstat, 3 * sizeof(double)));
+  model_refresh(m, ctx->stream);
   int nonpos = 0;
-  double ssum = 0.0;
-  CUDA_OK(ctx, cudaMemcpyAsync(&nonpos, dflag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_OK(ctx, cudaMemcpyAsync(&ssum, dsum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  CUDA_OK(ctx, cudaMemcpyAsync(&m.smin, dmin, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_OK(ctx, cudaMemcpyAsync(&nonpos, m.dstat, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_OK(ctx, cudaMemcpyAsync(&m.smin, m.dstat + 2, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
-  cudaFree(dflag);
   if (nonpos) {
     cudaFree(m.vel);
     cudaFree(m.slow);
+    cudaFree(m.dstat);
     return fail(ctx, EIK_ERR_ASSERT, "all(vel.>0.0)");
   }
   ctx->model_bytes += 2 * bytes;
@@ -277,15 +297,15 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     P.code = code + s * N;
     P.kL = kL + s * N;
     P.kd = kd + s * N;
-    {
-      // about one node's traveltime at the largest velocity
-      double dh[3];
-      node_dh(g, 0, dh);
-      double hmin = dh[0];
-      for (int a = 1; a < g.nd; a++) hmin = std::min(hmin, dh[a]);
-      P.delta = ctx->round_gate * hmin * m.smin;
-      P.incmin = 0.999 * (2.0 / 3.0) * hmin * m.smin / std::sqrt((double)g.nd);
-    }
+    P.delta = P.incmin = 0.0;  // set on the device from the model's smallest slowness
+  }
+  // round width: about one node's traveltime at the largest velocity, times round_gate
+  double hmin;
+  {
+    double dh[3];
+    node_dh(g, 0, dh);
+    hmin = dh[0];
+    for (int a = 1; a < g.nd; a++) hmin = std::min(hmin, dh[a]);
   }
   CoarseProblem* dp;
   GET(dp, CoarseProblem, "probs", nsrc);
@@ -339,16 +359,20 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     GET(ftie, uint8_t, "fine_tie", nsrc);
   }
 #undef GET
-  CUDA_OK(ctx, cudaMemcpyAsync(dp, hp.data(), sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
+  const void* hp_src = stage_host(ctx, hp.data(), sizeof(CoarseProblem) * nsrc);
+  if (!hp_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
+  CUDA_OK(ctx, cudaMemcpyAsync(dp, hp_src, sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
+  problem_scale_kernel<<<(int)((nsrc + 127) / 128), 128, 0, st>>>(dp, (int)nsrc, m.dstat + 2, ctx->round_gate, hmin,
+                                                                  g.nd);
   CUDA_OK(ctx, cudaMemsetAsync(fb.err, 0, sizeof(uint32_t) * 4, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.out, 0, sizeof(SrcOut) * nsrc, st));
-  cudaEventRecord(ctx->evk[0], st);
-  int nlaunch = 5;  // start-up, init, round init, seeds, solve
+  if (!ctx->capturing) cudaEventRecord(ctx->evk[0], st);
+  int nlaunch = 6;  // round widths, start-up, init, round init, seeds, solve
   if (refine && ctx->fine_replay) {
     launch_fine(fb, st);
   } else if (refine) {
     // the windows as round-solver problems, then the heap's stop reconstructed from keys
-    launch_fine_setup(fb, fprobs, m.smin, ctx->round_gate, fseed_lin, fseed_tt, fslow, fkL, fkd, st);
+    launch_fine_setup(fb, fprobs, m.dstat + 2, ctx->round_gate, fseed_lin, fseed_tt, fslow, fkL, fkd, st);
     SolveArgs fsa = sa;
     fsa.probs = fprobs;
     fsa.rs.stride = (unsigned long long)fb.nfmax;
@@ -356,34 +380,23 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     fsa.node_evals = sa.activations + 7;
     launch_rounds_init(fsa, st);
     launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
-    CUDA_OK(ctx, launch_coarse_solve(fsa, ctx->solve_sms(), st));
+    CUDA_OK(ctx, launch_coarse_solve(fsa, ctx->solve_sms(), ctx->ctas_per_sm, st));
     launch_fine_select(fb, fprobs, ftie, st);
+    // stops decided by exact ties: the heap is replayed for the flagged sources only, the
+    // flags staying on the device (no host round trip between the stages)
+    launch_fine_replay(fb, ftie, st);
     CUDA_OK(ctx, cudaGetLastError());
-    std::vector<uint8_t> tie(nsrc);
-    CUDA_OK(ctx, cudaMemcpyAsync(tie.data(), ftie, nsrc, cudaMemcpyDeviceToHost, st));
-    CUDA_OK(ctx, cudaStreamSynchronize(st));
-    std::vector<int32_t> list;
-    for (int64_t s = 0; s < nsrc; s++)
-      if (tie[s]) list.push_back((int32_t)s);
-    nlaunch += 6;
-    if (!list.empty()) {  // stops decided by exact ties: replay the heap for those sources
-      int32_t* dlist = (int32_t*)S.get("fine_replay_list", sizeof(int32_t) * list.size(), &rc);
-      if (!dlist) return fail(ctx, rc, "scratch allocation failed");
-      CUDA_OK(ctx, cudaMemcpyAsync(dlist, list.data(), sizeof(int32_t) * list.size(), cudaMemcpyHostToDevice, st));
-      launch_fine_replay(fb, dlist, (int)list.size(), st);
-      nlaunch += 1;
-    }
-    if (stats) stats->fine_replays += list.size();
+    nlaunch += 7;
   } else {
     launch_srcbox(fb, st);
   }
-  cudaEventRecord(ctx->evk[1], st);
+  if (!ctx->capturing) cudaEventRecord(ctx->evk[1], st);
   CUDA_OK(ctx, cudaGetLastError());
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
   CUDA_OK(ctx, cudaGetLastError());
-  cudaEventRecord(ctx->evk[2], st);
-  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->solve_sms(), st));
-  cudaEventRecord(ctx->evk[3], st);
+  if (!ctx->capturing) cudaEventRecord(ctx->evk[2], st);
+  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->solve_sms(), ctx->ctas_per_sm, st));
+  if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
   fw->fb = fb;
   fw->sa = sa;
@@ -393,6 +406,8 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   fw->kd = kd;
   fw->N = N;
   fw->nsrc = nsrc;
+  fw->fine_tie = (refine && !ctx->fine_replay) ? ftie : nullptr;
+  fw->launches = nlaunch;
   if (stats) stats->launches += nlaunch;
   return EIK_OK;
 }
@@ -408,6 +423,8 @@ int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
   cudaMemcpyAsync(&e, fw->fb.err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream);
   std::vector<SrcOut> outs(fw->nsrc);
   cudaMemcpyAsync(outs.data(), fw->fb.out, sizeof(SrcOut) * fw->nsrc, cudaMemcpyDeviceToHost, ctx->stream);
+  std::vector<uint8_t> tie(fw->fine_tie ? fw->nsrc : 0);
+  if (fw->fine_tie) cudaMemcpyAsync(tie.data(), fw->fine_tie, (size_t)fw->nsrc, cudaMemcpyDeviceToHost, ctx->stream);
   CUDA_OK(ctx, cudaStreamSynchronize(ctx->stream));
   uint32_t warn = 0;
   for (auto& o : outs) warn |= o.warn;
@@ -417,6 +434,7 @@ int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
     stats->tile_activations += ctr[2];
     stats->node_evals += ctr[3];
     stats->fwd_rounds += (uint64_t)rounds;
+    for (uint8_t f : tie) stats->fine_replays += f ? 1 : 0;
     for (int k = 0; k < 7; k++) stats->fwd_visits[k] += vis[k];
     float a = 0, b = 0;
     cudaEventElapsedTime(&a, ctx->evk[0], ctx->evk[1]);
@@ -472,11 +490,17 @@ int eik_ctx_create(int device, size_t hbm_budget, eik_ctx** out) {
 
 int eik_ctx_destroy(eik_ctx* ctx) {
   if (!ctx) return EIK_OK;
+  {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (ctx->live_plans > 0)
+      return fail(ctx, EIK_ERR_ASSERT, "context has %d live plan(s): destroy them first", ctx->live_plans);
+  }
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto& kv : ctx->models) {
     cudaFree(kv.second.vel);
     cudaFree(kv.second.slow);
+    cudaFree(kv.second.dstat);
   }
   ctx->scratch.release_all();
   cudaEventDestroy(ctx->ev0);
@@ -499,6 +523,12 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
   }
   if (std::strcmp(name, "fine_replay") == 0) {
     ctx->fine_replay = value != 0.0;
+    return EIK_OK;
+  }
+  if (std::strcmp(name, "ctas_per_sm") == 0) {
+    if (!(value >= 0.0 && value <= 32.0 && value == (double)(int)value))
+      return fail(ctx, EIK_ERR_ASSERT, "ctas_per_sm must be an integer in [0, 32]");
+    ctx->ctas_per_sm = (int)value;
     return EIK_OK;
   }
   if (std::strcmp(name, "sm_fraction") == 0) {
@@ -529,10 +559,14 @@ int eik_model_release(eik_ctx* ctx, eik_model_id model) {
   std::lock_guard<std::mutex> lk(ctx->mu);
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  if (it->second.plans > 0)
+    return fail(ctx, EIK_ERR_ASSERT, "model %lld is used by %d plan(s): destroy them first", (long long)model,
+                it->second.plans);
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaFree(it->second.vel);
   cudaFree(it->second.slow);
+  cudaFree(it->second.dstat);
   ctx->model_bytes -= 2 * sizeof(double) * (size_t)it->second.N;
   ctx->models.erase(it);
   return EIK_OK;

@@ -549,10 +549,11 @@ void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const doub
 }
 
 template <int ND>
-static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st) {
+static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
   const size_t sm = 0;
   int per = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND>, SOLVE_THREADS, sm);
+  if (ctas_per_sm > 0 && ctas_per_sm < per) per = ctas_per_sm;
   per = per < 1 ? 1 : per;
   SolveArgs args = sa;
   void* kargs[] = {&args};
@@ -561,8 +562,8 @@ static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, cudaStream_t st
                                      kargs, sm, st);
 }
 
-cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st) {
-  return sa.nd == 3 ? launch_solve_nd<3>(sa, nsm, st) : launch_solve_nd<2>(sa, nsm, st);
+cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
+  return sa.nd == 3 ? launch_solve_nd<3>(sa, nsm, ctas_per_sm, st) : launch_solve_nd<2>(sa, nsm, ctas_per_sm, st);
 }
 
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,

@@ -218,9 +218,10 @@ __device__ long long fine_window(const ForwardBatch& fb, const double* src, Fine
 constexpr int FINE_THREADS = 32;
 constexpr int MAXPOP = 128;
 
-__global__ void __launch_bounds__(FINE_THREADS) fine_fmm_kernel(ForwardBatch fb, const int32_t* srclist) {
+__global__ void __launch_bounds__(FINE_THREADS) fine_fmm_kernel(ForwardBatch fb, const uint8_t* only) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int s = srclist ? srclist[blockIdx.x] : blockIdx.x;
+  const int s = blockIdx.x;
+  if (only && !only[s]) return;  // replay of the flagged sources only
   const int lane = threadIdx.x;
   const GridDesc& g = fb.g;
   SrcOut& o = fb.out[s];
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(FINE_THREADS) fine_fmm_kernel(ForwardBatch fb,
 // node) does the heap's internal order decide; those sources are replayed exactly.
 
 // Window, fine source box, the fine problem of the round solver, its slowness and seeds.
-__global__ void fine_setup_kernel(ForwardBatch fb, CoarseProblem* fprobs, double smin, double gate,
+__global__ void fine_setup_kernel(ForwardBatch fb, CoarseProblem* fprobs, const double* dsmin, double gate,
                                   int32_t* fseed_lin, double* fseed_tt, double* fslow, double* fkL, uint8_t* fkd) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= fb.nsrc) return;
@@ -508,6 +509,7 @@ __global__ void fine_setup_kernel(ForwardBatch fb, CoarseProblem* fprobs, double
   node_dh(gf, 0, dh);
   double hmin = dh[0];
   for (int a = 1; a < gf.nd; a++) hmin = fmin(hmin, dh[a]);
+  const double smin = *dsmin;
   P.delta = gate * hmin * smin;
   P.incmin = 0.999 * (2.0 / 3.0) * hmin * smin / sqrt((double)gf.nd);
 }
@@ -780,10 +782,10 @@ __global__ void __launch_bounds__(SEL_THREADS) fine_select_kernel(ForwardBatch f
   }
 }
 
-void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, double smin, double gate,
+void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, const double* dsmin, double gate,
                        int32_t* fseed_lin, double* fseed_tt, double* fine_slow, double* fine_kL, uint8_t* fine_kd,
                        cudaStream_t st) {
-  fine_setup_kernel<<<(fb.nsrc + 63) / 64, 64, 0, st>>>(fb, fprobs, smin, gate, fseed_lin, fseed_tt, fine_slow,
+  fine_setup_kernel<<<(fb.nsrc + 63) / 64, 64, 0, st>>>(fb, fprobs, dsmin, gate, fseed_lin, fseed_tt, fine_slow,
                                                          fine_kL, fine_kd);
   fine_fill_kernel<<<592, 256, 0, st>>>(fb, fprobs);
 }
@@ -810,10 +812,10 @@ void launch_fine(const ForwardBatch& fb, cudaStream_t st) {
   fine_fmm_kernel<<<fb.nsrc, FINE_THREADS, sm, st>>>(fb, nullptr);
 }
 
-void launch_fine_replay(const ForwardBatch& fb, const int32_t* srclist, int n, cudaStream_t st) {
+void launch_fine_replay(const ForwardBatch& fb, const uint8_t* fine_tie, cudaStream_t st) {
   const size_t sm = fine_smem_bytes(fb.heapcap);
   cudaFuncSetAttribute(fine_fmm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  fine_fmm_kernel<<<n, FINE_THREADS, sm, st>>>(fb, srclist);
+  fine_fmm_kernel<<<fb.nsrc, FINE_THREADS, sm, st>>>(fb, fine_tie);
 }
 
 }  // namespace eik

@@ -110,12 +110,13 @@ void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const doub
 // Refined start-up as a fixed point: window set-up, the fine problems' arrays, the
 // acceptance set at the reference's stop, and the exact heap replay for the sources
 // whose stop is decided by a tie (flags in fine_tie, nonzero = replay needed).
-void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, double smin, double gate,
+void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, const double* dsmin, double gate,
                        int32_t* fseed_lin, double* fseed_tt, double* fine_slow, double* fine_kL, uint8_t* fine_kd,
                        cudaStream_t st);
 void launch_fine_select(const ForwardBatch& fb, const CoarseProblem* fprobs, uint8_t* fine_tie, cudaStream_t st);
-void launch_fine_replay(const ForwardBatch& fb, const int32_t* srclist, int n, cudaStream_t st);
-cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, cudaStream_t st);
+void launch_fine_replay(const ForwardBatch& fb, const uint8_t* fine_tie, cudaStream_t st);
+// ctas_per_sm: resident CTAs per SM of the persistent launch (0 = as many as fit)
+cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st);
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);
 // Gaussian smoothing of a gradient field (smoothgradkern = l, odd): weights on the host,

@@ -39,6 +39,8 @@ struct Model {
   double* vel = nullptr;   // device
   double* slow = nullptr;  // device, 1.0/vel
   double smin = 0.0;       // smallest slowness of the model (round width of the forward solve)
+  double* dstat = nullptr; // device: [non-positive flag, Σ slowness, smallest slowness]
+  int plans = 0;           // captured plans that hold this model's buffers
 };
 
 // Device results of the forward stage of one call.
@@ -51,6 +53,8 @@ struct ForwardState {
   uint8_t* kd = nullptr;
   long long N = 0;
   long long nsrc = 0;
+  const uint8_t* fine_tie = nullptr;  // per-source replay flags of the refined start-up (device)
+  int launches = 0;                   // kernels the forward stage launched
   std::vector<SrcOut> host_out;
 };
 
@@ -63,6 +67,30 @@ int check_positions(eik_ctx* ctx, const GridDesc& g, int64_t nsrc, const double*
                     const double* rec);
 int check_extra(eik_ctx* ctx, const eik_extra* ep);
 int err_to_rc(eik_ctx* ctx, uint32_t e);
+// Recomputes a model's slowness and its device statistics from its velocity (stream-ordered,
+// no host synchronisation, so it can be part of a captured graph).
+void model_refresh(const Model& m, cudaStream_t st);
+// Source of a host-to-device copy of `bytes` at `src` inside the pipeline: `src` itself, or,
+// while a plan is being captured, a pinned copy owned by the plan (a graph replays its
+// copies from the same host address, so that address must outlive the call).
+const void* stage_host(eik_ctx* ctx, const void* src, size_t bytes);
+
+// What is left to read back after a gradient pipeline has run: the forward's device state
+// and the adjoint's warning word and round counter.
+struct GradTail {
+  ForwardState fw;
+  uint32_t* dwarn = nullptr;
+  int32_t* arounds = nullptr;
+  int launches = 0;
+};
+int gradient_tail_stats(eik_ctx* ctx, GradTail& tail, eik_stats* stats);
+int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichgrad, const eik_extra& ep);
+// Forward + adjoint + assembly for nsrc sources whose inputs are on the device; outputs
+// (each nullable) stay on the device. tail_out (nullable) receives what to read back.
+int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
+                  const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
+                  const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit, eik_stats* stats,
+                  GradTail* tail_out);
 
 }  // namespace eik
 
@@ -73,6 +101,7 @@ struct eik_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // whole call
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
   double round_gate = 2.0;  // forward round width in units of (smallest spacing x smallest slowness)
+  int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
   double sm_fraction = 1.0; // share of the SMs the persistent (cooperative) solves of this context use
   bool fine_replay = false; // refined start-up by exact heap replay for every source (else only on ties)
   int solve_sms() const {
@@ -81,6 +110,9 @@ struct eik_ctx {
   }
   std::mutex mu;
   eik::Scratch scratch;
+  bool capturing = false;                    // the pipeline is being captured into a plan's graph
+  std::vector<void*>* stage_arena = nullptr; // pinned host copies made while capturing
+  int live_plans = 0;
   size_t model_bytes = 0;
   eik_model_id next_model = 0;
   std::map<eik_model_id, eik::Model> models;

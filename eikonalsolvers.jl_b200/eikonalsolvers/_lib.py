@@ -23,7 +23,7 @@ ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EI
 EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last_error",
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
             "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc",
-            "eik_ctx_set_param"]
+            "eik_ctx_set_param", "eik_plan_gradient", "eik_plan_run", "eik_plan_destroy"]
 
 
 class EikError(RuntimeError):
@@ -91,6 +91,12 @@ def load():
         L.eik_ctx_set_param.restype = C.c_int
         L.eik_ctx_stream.argtypes = [P]
         L.eik_ctx_stream.restype = C.c_void_p
+        L.eik_plan_gradient.argtypes = [P, C.c_int64, C.c_int64, P, P, P, C.c_int32, C.POINTER(eik_extra),
+                                        C.POINTER(P)]
+        L.eik_plan_run.argtypes = [P, P, P, P, P, P, P, C.POINTER(eik_stats)]
+        L.eik_plan_destroy.argtypes = [P]
+        for f in ("eik_plan_gradient", "eik_plan_run", "eik_plan_destroy"):
+            getattr(L, f).restype = C.c_int
         for f in ("eik_ctx_create", "eik_ctx_destroy", "eik_model_upload", "eik_model_upload_device",
                   "eik_model_release", "eik_traveltime", "eik_gradient", "eik_gradient_device"):
             getattr(L, f).restype = C.c_int

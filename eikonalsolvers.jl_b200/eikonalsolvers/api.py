@@ -71,6 +71,17 @@ class Context:
     def release(self, model: int):
         _lib.check(self.L.eik_model_release(self.h, C.c_int64(model)), self.h)
 
+    def plan_gradient(self, model: int, grd, coordsrc, coordrec, whichgrad, extraparams=None,
+                      nthreads: int = 1) -> "GradientPlan":
+        """Captures the gradient pipeline of this workload as a CUDA graph (GradientPlan)."""
+        return GradientPlan(self, model, grd, coordsrc, coordrec, whichgrad, extraparams, nthreads)
+
+    def autotune(self, model: int, grd, coordsrc, coordrec, extraparams=None, tuner=None, force: bool = False):
+        """Times the forward solve's launch parameters on this workload, keeps the fastest on
+        this context and returns the tuner's entry (eikonalsolvers.tune)."""
+        from .tune import default_tuner
+        return (tuner or default_tuner()).tune(self, model, grd, coordsrc, coordrec, extraparams, force)
+
     # ------------------------------------------------------------------ calls --
     def traveltime(self, model: int, grd, coordsrc, coordrec, returntt=False, extraparams=None):
         cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
@@ -140,6 +151,79 @@ class Context:
         if wg == "gradsrcloc":
             return gradsrc, float(misf[0])
         return gradvel, gradsrc, float(misf[0])
+
+
+class GradientPlan:
+    """A captured eik_gradient pipeline for fixed model, sources, receivers and parameters,
+    replayed with new velocities and observations (eik_plan_gradient / eik_plan_run).
+
+    ``run(pickobs, stdobs, vel=None)`` returns what ``Context.gradient`` returns; a ``vel``
+    replaces the model's velocity in place (it stays replaced). Results are bit-identical to
+    ``Context.gradient`` on the same inputs. Close the plan before releasing its model or
+    closing its context."""
+
+    def __init__(self, ctx: "Context", model: int, grd, coordsrc, coordrec, whichgrad, extraparams=None,
+                 nthreads: int = 1):
+        wg = whichgrad.lstrip(":") if isinstance(whichgrad, str) else whichgrad
+        assert wg in WHICHGRAD, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)"
+        self.ctx, self.grd, self.wg = ctx, grd, wg
+        cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+        if isinstance(coordrec, np.ndarray) and coordrec.dtype != object:
+            coordrec = [coordrec]
+        recs = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+        assert cs.shape[0] == len(recs), "size(coordsrc,1)==length(coordrec)"
+        self.nsrc = cs.shape[0]
+        self.nrec = [r.shape[0] for r in recs]
+        recoff = np.zeros(len(recs) + 1, dtype=np.int64)
+        for s, r in enumerate(recs):
+            recoff[s + 1] = recoff[s] + r.shape[0]
+        rec = np.ascontiguousarray(np.concatenate(recs, axis=0))
+        ep = _lib.extra_struct(extraparams, nthreads)
+        self.h = C.c_void_p()
+        _lib.check(ctx.L.eik_plan_gradient(ctx.h, C.c_int64(model), self.nsrc, _lib.ptr(cs), _lib.ptr(recoff),
+                                           _lib.ptr(rec), WHICHGRAD[wg], C.byref(ep), C.byref(self.h)), ctx.h)
+        self.last_stats = _lib.eik_stats()
+
+    def run(self, pickobs, stdobs, vel=None):
+        assert len(pickobs) == self.nsrc and len(stdobs) == self.nsrc, "length(coordrec)==length(pickobs)"
+        for n, p, s in zip(self.nrec, pickobs, stdobs):
+            assert np.asarray(p).shape[0] == n, "size(coordrec[r],1)==size(pickobs[r],1)"
+            assert np.asarray(s).shape == np.asarray(p).shape, "size(stdobs[r])==size(pickobs[r])"
+        po = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).ravel() for p in pickobs]))
+        so = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.float64).ravel() for p in stdobs]))
+        velf = None
+        if vel is not None:
+            vel = np.asarray(vel, dtype=np.float64)
+            assert tuple(vel.shape) == tuple(self.grd.grsize), "size(vel)==grd.grsize"
+            velf = np.ascontiguousarray(np.asfortranarray(vel).ravel(order="F"))
+        N = int(np.prod(self.grd.grsize))
+        nd = self.grd.ndim
+        gv = np.zeros(N, dtype=np.float64) if self.wg != "gradsrcloc" else None
+        gs = np.zeros(self.nsrc * nd, dtype=np.float64) if self.wg != "gradvel" else None
+        misf = np.zeros(1, dtype=np.float64)
+        st = _lib.eik_stats()
+        rc = self.ctx.L.eik_plan_run(self.h, _lib.ptr(velf), _lib.ptr(po), _lib.ptr(so), _lib.ptr(gv), _lib.ptr(gs),
+                                     _lib.ptr(misf), C.byref(st))
+        self.last_stats = st
+        _lib.check(rc, self.ctx.h)
+        gradvel = gv.reshape(self.grd.grsize, order="F") if gv is not None else None
+        gradsrc = gs.reshape(self.nsrc, nd) if gs is not None else None
+        if self.wg == "gradvel":
+            return gradvel, float(misf[0])
+        if self.wg == "gradsrcloc":
+            return gradsrc, float(misf[0])
+        return gradvel, gradsrc, float(misf[0])
+
+    def close(self):
+        if self.h:
+            self.ctx.L.eik_plan_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 _default: dict = {}

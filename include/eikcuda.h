@@ -124,8 +124,9 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * smallest slowness), default 2; "sm_fraction" = share of the SMs that the persistent
  * solve kernels of this context occupy, in (0, 1], default 1 (contexts whose calls overlap
  * on one GPU, as in a serving loop, each take a share so that their solves can be resident
- * together); "fine_replay" = 1 replays the refined start-up's heap for every source
- * instead of only where an exact tie decides its stop (default 0). Returns
+ * together); "ctas_per_sm" = resident CTAs per SM of the forward solve, an integer, 0 (the
+ * default) = as many as fit; "fine_replay" = 1 replays the refined start-up's heap for every
+ * source instead of only where an exact tie decides its stop (default 0). Returns
  * EIK_ERR_ASSERT for an unknown name or a value out of range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 
@@ -158,6 +159,26 @@ int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const do
                         const int64_t* rec_off, const double* rec_dev, const double* pickobs_dev,
                         const double* stdobs_dev, int32_t whichgrad, const eik_extra* ep,
                         double* gradvel_dev, double* gradsrc_dev, double* misfit_dev, eik_stats* stats);
+
+/* Captured gradient plans (no counterpart in the reference; for callers that evaluate
+ * eikgradient model after model with the same sources and receivers, as the HMC problem
+ * callables of HMCtraveltimes.jl:84-104 do). eik_plan_gradient validates like eik_gradient,
+ * runs the pipeline once and captures it as a CUDA graph for fixed model, sources,
+ * receivers, whichgrad and extraparams (and the context's scheduling parameters at that
+ * time). The plan owns its device buffers, taken from the context's HBM budget until
+ * eik_plan_destroy. eik_plan_run replays it: vel (host, column-major, nullable) replaces the
+ * model's velocity in place first (the model keeps it afterwards; NULL keeps the current
+ * one), pickobs/stdobs are the observations of this evaluation (rec_off[nsrc] values each);
+ * outputs as eik_gradient. Results are bit-identical to eik_gradient on the same inputs.
+ * While a plan exists its model cannot be released and its context cannot be destroyed
+ * (EIK_ERR_ASSERT). Replays of plans of one context are serialised with its other calls. */
+typedef struct eik_plan eik_plan;
+int eik_plan_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
+                      const int64_t* rec_off, const double* rec, int32_t whichgrad, const eik_extra* ep,
+                      eik_plan** out);
+int eik_plan_run(eik_plan* plan, const double* vel, const double* pickobs, const double* stdobs,
+                 double* gradvel, double* gradsrc, double* misfit, eik_stats* stats);
+int eik_plan_destroy(eik_plan* plan);
 
 /* No counterpart in the reference. Misfit 0.5*Σ_s Σ_r (t - obs)²/σ² of nsrc traveltime
  * grids that are already in device memory (ttgrids_dev: nsrc x N, as eik_traveltime
