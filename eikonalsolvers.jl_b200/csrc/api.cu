@@ -298,6 +298,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     P.kL = kL + s * N;
     P.kd = kd + s * N;
     P.delta = P.incmin = 0.0;  // set on the device from the model's smallest slowness
+    uniform_coeffs(g, &P.c1u, &P.c2u);
   }
   // round width: about one node's traveltime at the largest velocity, times round_gate
   double hmin;

@@ -1,16 +1,16 @@
 // Coarse-grid forward solve: the reference's heap-ordered FMM main loop
 // (ttFMM_core!, src/EikSolv/eikmainfwd.jl:427-823) restated as the fixed point of the
-// order rule of stencil.cuh and solved by a block-tiled active-node iteration.
+// order rule of stencil.cuh and solved by a node-level worklist iteration.
 //
-// One cooperative persistent launch serves many problems (sources, possibly of different
-// grids). It runs in rounds separated by a grid barrier. In round r each listed tile is
-// taken by one warp, which stages its traveltimes and keys plus a 2-node halo in shared
-// memory, evaluates its active nodes whose potential is below the problem's threshold
-// until nothing below it changes, writes the changed nodes back and marks the nodes of
-// the neighbouring tiles that read them for the next round. The threshold follows the
-// front (smallest pending potential + about one node's traveltime), so the rounds sweep
-// the grid in traveltime order. Every wait is bounded (global timer), the number of rounds
-// is bounded; both report through an error word instead of trapping.
+// One cooperative persistent launch serves many problems (the sources of a call, or the
+// refined windows around them). It runs in rounds separated by a grid barrier. In round r
+// the warps take the round's worklist 32 entries at a time; a node whose potential is at
+// most the problem's threshold is evaluated, and when its value or key changes the nodes
+// whose stencil reads it are listed for round r+1; a node still above the threshold is
+// listed again with its pending front. The threshold follows the front (smallest pending
+// front + a round width of about one node's traveltime), so the rounds sweep the grid in
+// traveltime order. Every wait is bounded (global timer), the number of rounds is bounded;
+// both report through an error word instead of trapping.
 #include "kernels.cuh"
 #include "rounds.cuh"
 
@@ -215,6 +215,8 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   nb_clear(nb);
   node_dh(g, c[0], nb.dh);
   nb.slow = __ldg(P.slow + l);
+  nb.c1u = P.c1u;
+  nb.c2u = P.c2u;
   // Lower bound of the node's value: every term of the local update is at least pot and
   // the quadratic adds at least (2/3) h s / sqrt(ND) (2nd-order coefficients 9/(4h^2)).
   // Until the round threshold reaches it the node cannot be final: no evaluation yet.
@@ -335,6 +337,7 @@ template <int ND>
 #endif
 __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_rounds_kernel(SolveArgs a) {
   const int lane = threadIdx.x & 31;
+  __shared__ unsigned long long wq[SOLVE_THREADS / 32][64];  // per-warp queue of entries to evaluate
   const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
   unsigned long long evals = 0;
 #ifdef EIK_PHASE
@@ -357,41 +360,68 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
     if (blockIdx.x == 0)
       for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
         thr_cur[p] = fmax(thr_prev[p], __longlong_as_double((long long)ld_volatile(nm + p)) + a.probs[p].delta);
-    for (;;) {
-      PH_T(tg);
-      unsigned int base = 0;
-      if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
-      base = __shfl_sync(0xffffffffu, base, 0);
-      PH_ADD(0, tg);
-      if (base >= n) break;
-      PH_T(tp);
-      const unsigned int idx = base + lane;
+    // Visits whose front still stands (nothing they read has changed) are settled when
+    // taken; the others wait in a per-warp queue in shared memory and are evaluated 32 at a
+    // time, so that a warp's lanes run the long evaluation path together.
+    unsigned long long* q = wq[threadIdx.x >> 5];
+    int qn = 0;  // queued entries (warp-uniform)
+    bool more = true;
+    while (more || qn > 0) {
       unsigned dirs = 0;
       double front = EIK_INF;
       int prob = 0;
       long long l = 0;
-      if (idx < n) {
-        const unsigned long long e = L[idx];
-        const unsigned int gid = (unsigned int)(e >> 32);
-        const double ef = (double)__uint_as_float((unsigned int)e);
-        prob = (int)(gid / N);
-        l = (long long)(gid - (unsigned long long)prob * N);
-        const CoarseProblem& P = a.probs[prob];
-        // window of one round width above the smallest pending front, never moving back
-        const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
-        const unsigned long long gb = (unsigned long long)prob * N;
-        if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
-          // still waiting and nothing it reads has changed: its front stands
-          front = ef;
-          dirs = 1u << DIR_SELF;
-          vk[0]++;
-        } else {
+      if (more && qn < 32) {
+        PH_T(tg);
+        unsigned int base = 0;
+        if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        PH_ADD(0, tg);
+        if (base >= n) {
+          more = false;
+          continue;
+        }
+        const unsigned int idx = base + lane;
+        bool queue = false;
+        unsigned long long e = 0;
+        if (idx < n) {
+          e = L[idx];
+          const unsigned int gid = (unsigned int)(e >> 32);
+          const double ef = (double)__uint_as_float((unsigned int)e);
+          prob = (int)(gid / N);
+          l = (long long)(gid - (unsigned long long)prob * N);
+          const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) +
+                                                    a.probs[prob].delta);
+          if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
+            front = ef;
+            dirs = 1u << DIR_SELF;
+            vk[0]++;
+          } else {
+            queue = true;
+          }
+        }
+        const unsigned qm = __ballot_sync(0xffffffffu, queue);
+        if (queue) q[qn + __popc(qm & ((1u << lane) - 1u))] = e;
+        qn += __popc(qm);
+        __syncwarp();
+      } else {
+        PH_T(tp);
+        const int k = qn < 32 ? qn : 32;
+        if (lane < k) {
+          const unsigned long long e = q[qn - k + lane];
+          const unsigned int gid = (unsigned int)(e >> 32);
+          prob = (int)(gid / N);
+          l = (long long)(gid - (unsigned long long)prob * N);
+          const CoarseProblem& P = a.probs[prob];
+          const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
+          const unsigned long long gb = (unsigned long long)prob * N;
           dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
                            : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
         }
+        qn -= k;
+        __syncwarp();
+        PH_ADD(1, tp);
       }
-      __syncwarp();
-      PH_ADD(1, tp);
       PH_T(ts);
       // list the next round's nodes once each (per-node round stamps)
       const CoarseProblem& P = a.probs[prob];

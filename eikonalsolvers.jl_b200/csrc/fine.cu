@@ -510,6 +510,7 @@ __global__ void fine_setup_kernel(ForwardBatch fb, CoarseProblem* fprobs, const 
   double hmin = dh[0];
   for (int a = 1; a < gf.nd; a++) hmin = fmin(hmin, dh[a]);
   const double smin = *dsmin;
+  uniform_coeffs(gf, &P.c1u, &P.c2u);
   P.delta = gate * hmin * smin;
   P.incmin = 0.999 * (2.0 / 3.0) * hmin * smin / sqrt((double)gf.nd);
 }

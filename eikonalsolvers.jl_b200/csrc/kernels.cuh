@@ -63,7 +63,20 @@ struct CoarseProblem {
   uint8_t* kd;     // key depth of special nodes
   double delta;    // round width of the forward solve (traveltime units)
   double incmin;   // smallest increment of the local update over a neighbour: (2/3) h s_min / sqrt(nd)
+  double c1u, c2u; // Cartesian grids: the local solver's coefficients 1/h^2 and 9/(4h^2); 0 otherwise
 };
+
+// The coefficients of a grid with the same spacing h on every axis, computed with the
+// local solver's own expressions (so they are the values it would compute per call).
+EIK_HD void uniform_coeffs(const GridDesc& g, double* c1u, double* c2u) {
+  if (is_cart(g)) {
+    const double h = g.spac[0];
+    *c1u = 1.0 / (h * h);
+    *c2u = 9.0 / (4.0 * (h * h));
+  } else {
+    *c1u = *c2u = 0.0;
+  }
+}
 
 // Worklists and thresholds of the round-synchronous forward solve. Nodes are numbered
 // globally over the problems of a call: problem * N + node.

@@ -81,6 +81,7 @@ struct Nbhd {
   uint32_t ok2;      // bit slot: 2nd order allowed on that side (!isonb2 of the distance-1 node)
   double dh[3];      // node spacing per axis
   double slow;       // 1/vel at the node (computed as 1.0/vel, as the reference)
+  double c1u, c2u;   // 1/h^2 and 9/(4h^2) when every axis has spacing h (else 0: per axis)
 };
 EIK_HD int slot(int a, int l) { return 2 * a + l; }
 EIK_HD Key nb_key1(const Nbhd& nb, int a, int l) {
@@ -102,6 +103,7 @@ EIK_HD void nb_clear(Nbhd& nb) {
       nb.L2[a][l] = EIK_INF;
     }
   nb.d1 = nb.d2 = nb.in1 = nb.ok2 = 0u;
+  nb.c1u = nb.c2u = 0.0;
 }
 
 // Fill one slot: distance-1 node inside the grid (t, key level L, depth d).
@@ -157,12 +159,12 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
     const double dh = nb.dh[a];
     if (use2 && use1) {
       const double tmpa2 = (1.0 / 3.0) * (4.0 * cv1 - cv2);
-      const double ca = 9.0 / (4.0 * (dh * dh));
+      const double ca = nb.c2u > 0.0 ? nb.c2u : 9.0 / (4.0 * (dh * dh));
       alpha += ca;
       beta += (-2.0 * ca) * tmpa2;
       gamma += ca * (tmpa2 * tmpa2);
     } else if (use1) {
-      const double ca = 1.0 / (dh * dh);
+      const double ca = nb.c1u > 0.0 ? nb.c1u : 1.0 / (dh * dh);
       alpha += ca;
       beta += (-2.0 * ca) * cv1;
       gamma += ca * (cv1 * cv1);
@@ -192,7 +194,7 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
       }
       if (use1) {
         const double dh = nb.dh[a];
-        const double ca = 1.0 / (dh * dh);
+        const double ca = nb.c1u > 0.0 ? nb.c1u : 1.0 / (dh * dh);
         alpha += ca;
         beta += (-2.0 * ca) * cv1;
         gamma += ca * (cv1 * cv1);
@@ -234,10 +236,11 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
     for (int a = 0; a < ND; a++) codes[a] = (a == id) ? cd[a] : (int8_t)0;
     return (dhid * nb.slow) + best;
   }
+  // The reference takes the larger of (-beta +- sqrt)/(2 alpha). alpha > 0 (at least one
+  // neighbour is used) and sqrt >= 0, and rounded addition and division by a positive number
+  // are monotone, so the '+' root is never below the '-' root: it is the larger one.
   const double tmpsq = sqrt(sqarg);
-  const double s1 = (-beta + tmpsq) / (2.0 * alpha);
-  const double s2 = (-beta - tmpsq) / (2.0 * alpha);
-  return (s2 > s1) ? s2 : s1;
+  return (-beta + tmpsq) / (2.0 * alpha);
 }
 
 // Smallest key of a reached in-grid immediate neighbour, strictly above lo if strict.
