@@ -259,6 +259,12 @@ def main_b200(args):
         w.pickobs[s0 + i] = p + rng.normal(0.0, 0.01, p.shape)
         w.stdobs[s0 + i] = 0.01 * np.ones(p.shape)
     mid = ctx.upload(w.vel, w.grd)
+    # launch parameters of this workload class from the autotuner's table (no timing here)
+    from eikonalsolvers.tune import default_tuner
+    tuned = default_tuner().apply_known(ctx, w.grd, nsrc, ep)
+    launch_params = ({"round_gate": tuned["round_gate"], "ctas_per_sm": tuned["ctas_per_sm"],
+                      "source": "autotuner table shipped with the package"} if tuned else
+                     {"round_gate": 2.0, "ctas_per_sm": 0, "source": "library defaults"})
     N = int(np.prod(w.grd.grsize))
     nd = w.grd.ndim
     cs, off, rec, po, so = flat_inputs(w, s0, s1)
@@ -347,6 +353,9 @@ def main_b200(args):
     plain = None
     if args.plain_sources > 0:
         npl = min(args.plain_sources, nsrc)
+        if not default_tuner().apply_known(ctx, w.grd, 1, ep):
+            ctx.set_param("round_gate", 2.0)
+            ctx.set_param("ctas_per_sm", 0)
         stp = _lib.eik_stats()
         offs = [np.array([0, off[i + 1] - off[i]], dtype=np.int64) for i in range(npl)]
         if ws > 1:
@@ -408,7 +417,8 @@ def main_b200(args):
                                    f"hgrid {w.grd.hgrid}, 4-layer model, {nsrc} sources per GPU, 400 receivers, "
                                    "default ExtraParams (refined start-up ds=5 r=3, smoothing radius 3)",
                        "sources_per_gpu": nsrc, "nodes": N, "parallelism": f"sources sharded over {ws} GPU(s)",
-                       "l2": "inputs and per-source fields far larger than L2 (no flush)"},
+                       "l2": "inputs and per-source fields far larger than L2 (no flush)",
+                       "launch_params": launch_params},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                     "steps": args.e2e_steps},
             "plain": plain,

@@ -14,7 +14,9 @@ This loop serves such callers from many threads or processes on one GPU:
   run as one batched call and the picks are split back per request;
 * a request that does not fit a slot's HBM budget fails alone (EIK_ERR_OUT_OF_BUDGET);
 * latency (submission to completion) is recorded per request; `stats()` gives p50/p99 and
-  source-solves/s.
+  source-solves/s;
+* each call runs with the launch parameters the autotuner's table holds for its workload
+  class (the library defaults otherwise).
 
 Results do not depend on the mix: the forward traveltimes are the unique fixed point of
 the order rule whatever the batch, and gradient requests are never merged (their
@@ -34,6 +36,7 @@ import numpy as np
 
 from .api import Context
 from .structs import ExtraParams
+from .tune import default_tuner
 
 
 @dataclass
@@ -68,8 +71,10 @@ class Server:
     """Serves `Request`s on one GPU with `slots` concurrent worker contexts."""
 
     def __init__(self, device: int = 0, slots: int = 2, hbm_budget_per_slot: int = 0,
-                 max_batch_sources: int = 64, context_factory=None):
+                 max_batch_sources: int = 64, context_factory=None, tuner=None):
         self.slots = max(1, int(slots))
+        # launch parameters per workload class (autotuner table; results do not depend on them)
+        self.tuner = tuner if tuner is not None else default_tuner()
         self.max_batch_sources = int(max_batch_sources)
         make = context_factory or (lambda: Context(device, hbm_budget_per_slot))
         self._ctx = []
@@ -151,6 +156,10 @@ class Server:
             try:
                 grd = self._models[batch[0].model][1]
                 mid = self._model_id(slot, batch[0].model)
+                nsrc = sum(r.nsrc for r in batch)
+                if not self.tuner.apply_known(ctx, grd, nsrc, batch[0].extraparams):
+                    ctx.set_param("round_gate", 2.0)
+                    ctx.set_param("ctas_per_sm", 0)
                 if batch[0].kind == "traveltime":
                     cs = np.vstack([np.atleast_2d(r.coordsrc) for r in batch])
                     recs = [rr for r in batch for rr in r.coordrec]

@@ -16,7 +16,9 @@ the workload's shape class (dimension, node count and source count rounded up to
 two, refined start-up or not). Later calls with a workload of the same class reuse the
 entry without timing. The table can be kept in a JSON file (``path``, or the
 ``EIK_TUNE_CACHE`` environment variable) so that a serving process or a sampler starts
-tuned.
+tuned. Below the caller's table sits the table shipped with the package
+(``tuned_b200.json``: entries measured by ``Tuner.tune`` on a B200 for the standard
+workloads), consulted when the caller's table has no entry for a class.
 """
 from __future__ import annotations
 
@@ -29,6 +31,7 @@ from typing import Dict, Iterable, Optional, Sequence
 import numpy as np
 
 DEFAULT_CANDIDATES: Dict[str, Sequence[float]] = {"round_gate": (1.0, 2.0, 3.0), "ctas_per_sm": (2, 3, 4)}
+SHIPPED_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_b200.json")
 
 
 def _pow2(n: int) -> int:
@@ -45,12 +48,16 @@ class Tuner:
     """Table of tuned launch parameters per workload class, optionally kept in a JSON file."""
 
     def __init__(self, path: Optional[str] = None, candidates: Optional[Dict[str, Iterable[float]]] = None,
-                 repeats: int = 2):
+                 repeats: int = 2, shipped: Optional[str] = SHIPPED_TABLE):
         self.path = path if path is not None else os.environ.get("EIK_TUNE_CACHE")
         self.candidates = {k: tuple(v) for k, v in (candidates or DEFAULT_CANDIDATES).items()}
         self.repeats = max(1, int(repeats))
         self.table: Dict[str, dict] = {}
+        self.base: Dict[str, dict] = {}
         self._lock = threading.Lock()
+        if shipped and os.path.exists(shipped):
+            with open(shipped) as f:
+                self.base = json.load(f)
         if self.path and os.path.exists(self.path):
             with open(self.path) as f:
                 self.table = json.load(f)
@@ -68,17 +75,27 @@ class Tuner:
         ctx.set_param("round_gate", float(entry["round_gate"]))
         ctx.set_param("ctas_per_sm", float(entry["ctas_per_sm"]))
 
-    def lookup(self, grd, nsrc: int, extraparams=None) -> Optional[dict]:
+    def _get(self, key: str) -> Optional[dict]:
         with self._lock:
-            return self.table.get(workload_key(grd, nsrc, extraparams))
+            e = self.table.get(key)
+        return e if e is not None else self.base.get(key)
+
+    def lookup(self, grd, nsrc: int, extraparams=None) -> Optional[dict]:
+        return self._get(workload_key(grd, nsrc, extraparams))
+
+    def apply_known(self, ctx, grd, nsrc: int, extraparams=None) -> Optional[dict]:
+        """Applies the table's entry for this workload class, if any (no timing)."""
+        e = self.lookup(grd, nsrc, extraparams)
+        if e is not None:
+            self.apply(ctx, e)
+        return e
 
     def tune(self, ctx, model: int, grd, coordsrc, coordrec, extraparams=None, force: bool = False) -> dict:
         """Sets the fastest (round_gate, ctas_per_sm) for this workload on ``ctx`` and returns
         the table entry: {"round_gate", "ctas_per_sm", "ms", "timings"}."""
         nsrc = int(np.atleast_2d(coordsrc).shape[0])
         key = workload_key(grd, nsrc, extraparams)
-        with self._lock:
-            entry = self.table.get(key)
+        entry = self._get(key)
         if entry is not None and not force:
             self.apply(ctx, entry)
             return entry

@@ -45,7 +45,8 @@ REC = [np.array([[1.0, 1.0]])] * 2
 
 def test_tuner_picks_the_fastest_and_reuses_it(tmp_path):
     path = str(tmp_path / "tune.json")
-    t = Tuner(path=path, candidates={"round_gate": (1.0, 2.0, 3.0), "ctas_per_sm": (2, 3, 4)}, repeats=2)
+    t = Tuner(path=path, candidates={"round_gate": (1.0, 2.0, 3.0), "ctas_per_sm": (2, 3, 4)}, repeats=2,
+              shipped=None)
     ctx = FakeContext(lambda g, c: 1.0 + abs(g - 2.0) + 0.5 * abs(c - 3))
     e = t.tune(ctx, 0, GRD, CS, REC)
     assert (e["round_gate"], e["ctas_per_sm"]) == (2.0, 3)
@@ -64,11 +65,11 @@ def test_tuner_picks_the_fastest_and_reuses_it(tmp_path):
     t.tune(FakeContext(lambda g, c: c), 0, GRD, np.zeros((5, 2)), REC * 3)
     table = json.load(open(path))
     assert len(table) == 2
-    assert Tuner(path=path).lookup(GRD, 5)["ctas_per_sm"] == 2
+    assert Tuner(path=path, shipped=None).lookup(GRD, 5)["ctas_per_sm"] == 2
 
 
 def test_tuner_refuses_schedule_dependent_results():
-    t = Tuner(path="", candidates={"round_gate": (1.0, 2.0), "ctas_per_sm": (4,)}, repeats=1)
+    t = Tuner(path="", candidates={"round_gate": (1.0, 2.0), "ctas_per_sm": (4,)}, repeats=1, shipped=None)
     ctx = FakeContext(lambda g, c: 1.0, picks_for=lambda p: [np.arange(3.0) * p["round_gate"]])
     with pytest.raises(RuntimeError, match="schedule independent"):
         t.tune(ctx, 0, GRD, CS, REC)
@@ -81,7 +82,7 @@ def test_tuner_on_the_gpu(tmp_path):
     ctx, ref = Context(0), Context(0)
     try:
         mid, mref = ctx.upload(w.vel, w.grd), ref.upload(w.vel, w.grd)
-        t = Tuner(path=str(tmp_path / "t.json"), repeats=1)
+        t = Tuner(path=str(tmp_path / "t.json"), repeats=1, shipped=None)
         e = ctx.autotune(mid, w.grd, w.coordsrc, w.coordrec, tuner=t)
         assert len(e["timings"]) == 9 and e["ms"] == min(x[2] for x in e["timings"])
         got = ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec)
@@ -90,3 +91,20 @@ def test_tuner_on_the_gpu(tmp_path):
     finally:
         ctx.close()
         ref.close()
+
+
+def test_shipped_table_covers_the_standard_workloads():
+    """The table shipped with the package (measured on a B200 by Tuner.tune) has entries for
+    the 256^3 x 32-source 3D workload and the 1024 x 640 x 64-source 2D workload, each one of
+    the timed candidates, and the caller's own table takes precedence over it."""
+    t = Tuner(path="")
+    for w, n in ((CF.cfg3(scale=1.0, nsrc=1, nrec_side=2), 32), (CF.cfg2(scale=1.0, nsrc=1), 64)):
+        e = t.lookup(w.grd, n, ExtraParams())
+        assert e is not None
+        assert [e["round_gate"], e["ctas_per_sm"], e["ms"]] in e["timings"]
+        ctx = FakeContext(lambda g, c: 1.0)
+        assert t.apply_known(ctx, w.grd, n, ExtraParams()) == e
+        assert ctx.params == {"round_gate": e["round_gate"], "ctas_per_sm": float(e["ctas_per_sm"])}
+    own = Tuner(path="")
+    own.table[workload_key(CF.cfg2(scale=1.0, nsrc=1).grd, 64)] = {"round_gate": 9.0, "ctas_per_sm": 1}
+    assert own.lookup(CF.cfg2(scale=1.0, nsrc=1).grd, 64)["round_gate"] == 9.0
