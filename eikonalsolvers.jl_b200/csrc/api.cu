@@ -381,7 +381,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     fsa.node_evals = sa.activations + 7;
     launch_rounds_init(fsa, st);
     launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
-    CUDA_OK(ctx, launch_coarse_solve(fsa, ctx->solve_sms(), ctx->ctas_per_sm, st));
+    CUDA_OK(ctx, launch_coarse_solve(fsa, ctx->solve_sms(), ctx->ctas_per_sm, ctx->fwd_queue, st));
     launch_fine_select(fb, fprobs, ftie, st);
     // stops decided by exact ties: the heap is replayed for the flagged sources only, the
     // flags staying on the device (no host round trip between the stages)
@@ -396,7 +396,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
   CUDA_OK(ctx, cudaGetLastError());
   if (!ctx->capturing) cudaEventRecord(ctx->evk[2], st);
-  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->solve_sms(), ctx->ctas_per_sm, st));
+  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->solve_sms(), ctx->ctas_per_sm, ctx->fwd_queue, st));
   if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
   fw->fb = fb;
@@ -530,6 +530,12 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
     if (!(value >= 0.0 && value <= 32.0 && value == (double)(int)value))
       return fail(ctx, EIK_ERR_ASSERT, "ctas_per_sm must be an integer in [0, 32]");
     ctx->ctas_per_sm = (int)value;
+    return EIK_OK;
+  }
+  if (std::strcmp(name, "fwd_queue") == 0) {
+    if (!(value == -1.0 || value == 0.0 || value == 1.0))
+      return fail(ctx, EIK_ERR_ASSERT, "fwd_queue must be -1 (automatic), 0 or 1");
+    ctx->fwd_queue = (int)value;
     return EIK_OK;
   }
   if (std::strcmp(name, "sm_fraction") == 0) {

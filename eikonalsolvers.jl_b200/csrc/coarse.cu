@@ -331,13 +331,20 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
 // follow the front like a Dijkstra sweep with buckets one node wide. A node whose value or
 // key changed lists the nodes whose stencil reads it for the next round; a node below the
 // front is listed again. The result is the same fixed point as any other evaluation order.
-template <int ND>
+//
+// QUEUE selects how a warp works through its entries: true settles the visits whose front
+// still stands at once and queues the others in shared memory, evaluating them 32 at a time
+// (the lanes of a warp then run the long evaluation path together, and the later
+// evaluation sees more final neighbours); false evaluates each lane's entry in place. The
+// queue pays on large rounds; on small ones a warp left holding queued entries at the end
+// of a round keeps the others waiting at the barrier.
 #ifndef EIK_FWD_MINBLOCKS
 #define EIK_FWD_MINBLOCKS 4  // CTAs per SM the register budget is sized for
 #endif
+template <int ND, bool QUEUE>
 __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_rounds_kernel(SolveArgs a) {
   const int lane = threadIdx.x & 31;
-  __shared__ unsigned long long wq[SOLVE_THREADS / 32][64];  // per-warp queue of entries to evaluate
+  __shared__ unsigned long long wq[SOLVE_THREADS / 32][QUEUE ? 64 : 1];  // per-warp queue of entries to evaluate
   const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
   unsigned long long evals = 0;
 #ifdef EIK_PHASE
@@ -360,123 +367,218 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
     if (blockIdx.x == 0)
       for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
         thr_cur[p] = fmax(thr_prev[p], __longlong_as_double((long long)ld_volatile(nm + p)) + a.probs[p].delta);
-    // Visits whose front still stands (nothing they read has changed) are settled when
-    // taken; the others wait in a per-warp queue in shared memory and are evaluated 32 at a
-    // time, so that a warp's lanes run the long evaluation path together.
-    unsigned long long* q = wq[threadIdx.x >> 5];
-    int qn = 0;  // queued entries (warp-uniform)
-    bool more = true;
-    while (more || qn > 0) {
-      unsigned dirs = 0;
-      double front = EIK_INF;
-      int prob = 0;
-      long long l = 0;
-      if (more && qn < 32) {
+    if constexpr (QUEUE) {
+      // Visits whose front still stands (nothing they read has changed) are settled when
+      // taken; the others wait in a per-warp queue in shared memory and are evaluated 32 at a
+      // time, so that a warp's lanes run the long evaluation path together.
+      unsigned long long* q = wq[threadIdx.x >> 5];
+      int qn = 0;  // queued entries (warp-uniform)
+      bool more = true;
+      while (more || qn > 0) {
+        unsigned dirs = 0;
+        double front = EIK_INF;
+        int prob = 0;
+        long long l = 0;
+        if (more && qn < 32) {
+          PH_T(tg);
+          unsigned int base = 0;
+          if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
+          base = __shfl_sync(0xffffffffu, base, 0);
+          PH_ADD(0, tg);
+          if (base >= n) {
+            more = false;
+            continue;
+          }
+          const unsigned int idx = base + lane;
+          bool queue = false;
+          unsigned long long e = 0;
+          if (idx < n) {
+            e = L[idx];
+            const unsigned int gid = (unsigned int)(e >> 32);
+            const double ef = (double)__uint_as_float((unsigned int)e);
+            prob = (int)(gid / N);
+            l = (long long)(gid - (unsigned long long)prob * N);
+            const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) +
+                                                      a.probs[prob].delta);
+            if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
+              front = ef;
+              dirs = 1u << DIR_SELF;
+              vk[0]++;
+            } else {
+              queue = true;
+            }
+          }
+          const unsigned qm = __ballot_sync(0xffffffffu, queue);
+          if (queue) q[qn + __popc(qm & ((1u << lane) - 1u))] = e;
+          qn += __popc(qm);
+          __syncwarp();
+        } else {
+          PH_T(tp);
+          const int k = qn < 32 ? qn : 32;
+          if (lane < k) {
+            const unsigned long long e = q[qn - k + lane];
+            const unsigned int gid = (unsigned int)(e >> 32);
+            prob = (int)(gid / N);
+            l = (long long)(gid - (unsigned long long)prob * N);
+            const CoarseProblem& P = a.probs[prob];
+            const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
+            const unsigned long long gb = (unsigned long long)prob * N;
+            dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
+                             : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
+          }
+          qn -= k;
+          __syncwarp();
+          PH_ADD(1, tp);
+        }
+        PH_T(ts);
+        // list the next round's nodes once each (per-node round stamps)
+        const CoarseProblem& P = a.probs[prob];
+        const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
+                          (int)(l / ((long long)P.g.n[0] * P.g.n[1]))};
+        const unsigned long long gbase = (unsigned long long)prob * N;
+        unsigned keep = 0;
+        for (int k = 0; k <= DIR_SELF; k++) {
+          if (!((dirs >> k) & 1u)) continue;
+          long long nl = l;
+          if (k != DIR_SELF) {
+            int p[3] = {c[0], c[1], c[2]};
+            p[k >> 2] += dir_off(k);
+            nl = lin3(P.g, p[0], p[1], p[2]);
+          }
+          if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
+        }
+        __syncwarp();
+        PH_ADD(2, ts);
+        PH_T(ta);
+        // warp-aggregated append: one atomic per 32 nodes
+        const int cntl = __popc(keep);
+        int incl = cntl;
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned int wbase = 0;
+        if (lane == 0 && total) wbase = atomicAdd(a.rs.cnt + nb3, (unsigned int)total);
+        wbase = __shfl_sync(0xffffffffu, wbase, 0) + (unsigned int)(incl - cntl);
+        for (int k = 0; k <= DIR_SELF; k++) {
+          if (!((keep >> k) & 1u)) continue;
+          long long nl = l;
+          if (k != DIR_SELF) {
+            int p[3] = {c[0], c[1], c[2]};
+            p[k >> 2] += dir_off(k);
+            nl = lin3(P.g, p[0], p[1], p[2]);
+          }
+          Lnext[wbase++] = list_entry((unsigned int)(gbase + nl), front);
+        }
+        {
+          // one update per problem and warp: the lanes of a problem agree on their smallest front
+          const double fv = keep ? front : EIK_INF;
+          const unsigned grp = __match_any_sync(0xffffffffu, prob);
+          double gmin = fv;
+          for (unsigned m = grp; m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            gmin = fmin(gmin, __shfl_sync(grp, fv, src));
+          }
+          if (lane == __ffs(grp) - 1) atomic_min_pos(nmn + prob, gmin);
+        }
+        __syncwarp();
+        PH_ADD(3, ta);
+      }
+    } else {
+      // every lane evaluates its own entry in place
+      for (;;) {
         PH_T(tg);
         unsigned int base = 0;
         if (lane == 0) base = atomicAdd(a.rs.grab + b3, 32u);
         base = __shfl_sync(0xffffffffu, base, 0);
         PH_ADD(0, tg);
-        if (base >= n) {
-          more = false;
-          continue;
-        }
+        if (base >= n) break;
+        PH_T(tp);
         const unsigned int idx = base + lane;
-        bool queue = false;
-        unsigned long long e = 0;
+        unsigned dirs = 0;
+        double front = EIK_INF;
+        int prob = 0;
+        long long l = 0;
         if (idx < n) {
-          e = L[idx];
+          const unsigned long long e = L[idx];
           const unsigned int gid = (unsigned int)(e >> 32);
           const double ef = (double)__uint_as_float((unsigned int)e);
           prob = (int)(gid / N);
           l = (long long)(gid - (unsigned long long)prob * N);
-          const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) +
-                                                    a.probs[prob].delta);
+          const CoarseProblem& P = a.probs[prob];
+          // window of one round width above the smallest pending front, never moving back
+          const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
+          const unsigned long long gb = (unsigned long long)prob * N;
           if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
+            // still waiting and nothing it reads has changed: its front stands
             front = ef;
             dirs = 1u << DIR_SELF;
             vk[0]++;
           } else {
-            queue = true;
+            dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
+                             : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
           }
         }
-        const unsigned qm = __ballot_sync(0xffffffffu, queue);
-        if (queue) q[qn + __popc(qm & ((1u << lane) - 1u))] = e;
-        qn += __popc(qm);
-        __syncwarp();
-      } else {
-        PH_T(tp);
-        const int k = qn < 32 ? qn : 32;
-        if (lane < k) {
-          const unsigned long long e = q[qn - k + lane];
-          const unsigned int gid = (unsigned int)(e >> 32);
-          prob = (int)(gid / N);
-          l = (long long)(gid - (unsigned long long)prob * N);
-          const CoarseProblem& P = a.probs[prob];
-          const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
-          const unsigned long long gb = (unsigned long long)prob * N;
-          dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
-                           : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
-        }
-        qn -= k;
         __syncwarp();
         PH_ADD(1, tp);
-      }
-      PH_T(ts);
-      // list the next round's nodes once each (per-node round stamps)
-      const CoarseProblem& P = a.probs[prob];
-      const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
-                        (int)(l / ((long long)P.g.n[0] * P.g.n[1]))};
-      const unsigned long long gbase = (unsigned long long)prob * N;
-      unsigned keep = 0;
-      for (int k = 0; k <= DIR_SELF; k++) {
-        if (!((dirs >> k) & 1u)) continue;
-        long long nl = l;
-        if (k != DIR_SELF) {
-          int p[3] = {c[0], c[1], c[2]};
-          p[k >> 2] += dir_off(k);
-          nl = lin3(P.g, p[0], p[1], p[2]);
+        PH_T(ts);
+        // list the next round's nodes once each (per-node round stamps)
+        const CoarseProblem& P = a.probs[prob];
+        const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
+                          (int)(l / ((long long)P.g.n[0] * P.g.n[1]))};
+        const unsigned long long gbase = (unsigned long long)prob * N;
+        unsigned keep = 0;
+        for (int k = 0; k <= DIR_SELF; k++) {
+          if (!((dirs >> k) & 1u)) continue;
+          long long nl = l;
+          if (k != DIR_SELF) {
+            int p[3] = {c[0], c[1], c[2]};
+            p[k >> 2] += dir_off(k);
+            nl = lin3(P.g, p[0], p[1], p[2]);
+          }
+          if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
         }
-        if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
-      }
-      __syncwarp();
-      PH_ADD(2, ts);
-      PH_T(ta);
-      // warp-aggregated append: one atomic per 32 nodes
-      const int cntl = __popc(keep);
-      int incl = cntl;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      unsigned int wbase = 0;
-      if (lane == 0 && total) wbase = atomicAdd(a.rs.cnt + nb3, (unsigned int)total);
-      wbase = __shfl_sync(0xffffffffu, wbase, 0) + (unsigned int)(incl - cntl);
-      for (int k = 0; k <= DIR_SELF; k++) {
-        if (!((keep >> k) & 1u)) continue;
-        long long nl = l;
-        if (k != DIR_SELF) {
-          int p[3] = {c[0], c[1], c[2]};
-          p[k >> 2] += dir_off(k);
-          nl = lin3(P.g, p[0], p[1], p[2]);
+        __syncwarp();
+        PH_ADD(2, ts);
+        PH_T(ta);
+        // warp-aggregated append: one atomic per 32 nodes
+        const int cntl = __popc(keep);
+        int incl = cntl;
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
         }
-        Lnext[wbase++] = list_entry((unsigned int)(gbase + nl), front);
-      }
-      {
-        // one update per problem and warp: the lanes of a problem agree on their smallest front
-        const double fv = keep ? front : EIK_INF;
-        const unsigned grp = __match_any_sync(0xffffffffu, prob);
-        double gmin = fv;
-        for (unsigned m = grp; m; m &= m - 1) {
-          const int src = __ffs(m) - 1;
-          gmin = fmin(gmin, __shfl_sync(grp, fv, src));
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned int wbase = 0;
+        if (lane == 0 && total) wbase = atomicAdd(a.rs.cnt + nb3, (unsigned int)total);
+        wbase = __shfl_sync(0xffffffffu, wbase, 0) + (unsigned int)(incl - cntl);
+        for (int k = 0; k <= DIR_SELF; k++) {
+          if (!((keep >> k) & 1u)) continue;
+          long long nl = l;
+          if (k != DIR_SELF) {
+            int p[3] = {c[0], c[1], c[2]};
+            p[k >> 2] += dir_off(k);
+            nl = lin3(P.g, p[0], p[1], p[2]);
+          }
+          Lnext[wbase++] = list_entry((unsigned int)(gbase + nl), front);
         }
-        if (lane == __ffs(grp) - 1) atomic_min_pos(nmn + prob, gmin);
+        {
+          // one update per problem and warp: the lanes of a problem agree on their smallest front
+          const double fv = keep ? front : EIK_INF;
+          const unsigned grp = __match_any_sync(0xffffffffu, prob);
+          double gmin = fv;
+          for (unsigned m = grp; m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            gmin = fmin(gmin, __shfl_sync(grp, fv, src));
+          }
+          if (lane == __ffs(grp) - 1) atomic_min_pos(nmn + prob, gmin);
+        }
+        __syncwarp();
+        PH_ADD(3, ta);
       }
-      __syncwarp();
-      PH_ADD(3, ta);
     }
     // buffers of round r+2 (last used in round r-1)
     if (blockIdx.x == 0) {
@@ -578,22 +680,26 @@ void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const doub
   else seed_kernel<2><<<sa.nprob, 128, 0, st>>>(sa, seed_lin, seed_tt, out, fine_corners ? 1 : 0, seedcap);
 }
 
-template <int ND>
+template <int ND, bool QUEUE>
 static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
   const size_t sm = 0;
   int per = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND>, SOLVE_THREADS, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND, QUEUE>, SOLVE_THREADS, sm);
   if (ctas_per_sm > 0 && ctas_per_sm < per) per = ctas_per_sm;
   per = per < 1 ? 1 : per;
   SolveArgs args = sa;
   void* kargs[] = {&args};
   // cooperative: every CTA is resident, so the grid barrier between rounds cannot deadlock
-  return cudaLaunchCooperativeKernel((const void*)coarse_rounds_kernel<ND>, dim3(nsm * per), dim3(SOLVE_THREADS),
-                                     kargs, sm, st);
+  return cudaLaunchCooperativeKernel((const void*)coarse_rounds_kernel<ND, QUEUE>, dim3(nsm * per),
+                                     dim3(SOLVE_THREADS), kargs, sm, st);
 }
 
-cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
-  return sa.nd == 3 ? launch_solve_nd<3>(sa, nsm, ctas_per_sm, st) : launch_solve_nd<2>(sa, nsm, ctas_per_sm, st);
+cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, int queue, cudaStream_t st) {
+  // automatic choice: the queue from 2^27 node-sources per launch (256^3 x 8 sources) up
+  const bool q = queue > 0 || (queue < 0 && (unsigned long long)sa.nprob * sa.rs.stride >= (1ull << 27));
+  if (sa.nd == 3)
+    return q ? launch_solve_nd<3, true>(sa, nsm, ctas_per_sm, st) : launch_solve_nd<3, false>(sa, nsm, ctas_per_sm, st);
+  return q ? launch_solve_nd<2, true>(sa, nsm, ctas_per_sm, st) : launch_solve_nd<2, false>(sa, nsm, ctas_per_sm, st);
 }
 
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,

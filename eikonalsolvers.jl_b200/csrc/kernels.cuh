@@ -128,8 +128,9 @@ void launch_fine_setup(const ForwardBatch& fb, CoarseProblem* fprobs, const doub
                        cudaStream_t st);
 void launch_fine_select(const ForwardBatch& fb, const CoarseProblem* fprobs, uint8_t* fine_tie, cudaStream_t st);
 void launch_fine_replay(const ForwardBatch& fb, const uint8_t* fine_tie, cudaStream_t st);
-// ctas_per_sm: resident CTAs per SM of the persistent launch (0 = as many as fit)
-cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st);
+// ctas_per_sm: resident CTAs per SM of the persistent launch (0 = as many as fit);
+// queue: per-warp evaluation queue 1 = on, 0 = off, -1 = chosen by the launch's size
+cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, int queue, cudaStream_t st);
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);
 // Gaussian smoothing of a gradient field (smoothgradkern = l, odd): weights on the host,

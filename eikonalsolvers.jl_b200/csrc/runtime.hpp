@@ -102,6 +102,7 @@ struct eik_ctx {
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
   double round_gate = 2.0;  // forward round width in units of (smallest spacing x smallest slowness)
   int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
+  int fwd_queue = -1;        // per-warp evaluation queue of the forward solve: -1 by size, 0 off, 1 on
   double sm_fraction = 1.0; // share of the SMs the persistent (cooperative) solves of this context use
   bool fine_replay = false; // refined start-up by exact heap replay for every source (else only on ties)
   int solve_sms() const {
