@@ -4,8 +4,8 @@ Python mirror of the reference's public API over the C-ABI library libeikcuda.so
 """
 from .structs import (ExtraParams, Grid2DCart, Grid2DSphere, Grid3DCart, Grid3DSphere,
                       GridRefinementPars, JuliaRange)
-from .api import Context, GradientPlan, default_context, eikgradient, eiktraveltime, eikttimemisfit
+from .api import Context, GradientPlan, default_context, eikgradient, eiktraveltime, eikttimemisfit, tracerays
 
 __all__ = ["Grid2DCart", "Grid3DCart", "Grid2DSphere", "Grid3DSphere", "ExtraParams",
            "GridRefinementPars", "JuliaRange", "Context", "GradientPlan", "default_context", "eiktraveltime",
-           "eikgradient", "eikttimemisfit"]
+           "eikgradient", "eikttimemisfit", "tracerays"]

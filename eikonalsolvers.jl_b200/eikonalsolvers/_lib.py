@@ -23,7 +23,8 @@ ERRORS = {-1: "EIK_ERR_ASSERT", -2: "EIK_ERR_ERROR", -3: "EIK_ERR_CUDA", -4: "EI
 EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last_error",
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
             "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc",
-            "eik_ctx_set_param", "eik_plan_gradient", "eik_plan_run", "eik_plan_destroy"]
+            "eik_ctx_set_param", "eik_plan_gradient", "eik_plan_run", "eik_plan_destroy", "eik_tracerays",
+            "eik_traveltime_rays"]
 
 
 class EikError(RuntimeError):
@@ -95,7 +96,11 @@ def load():
                                         C.POINTER(P)]
         L.eik_plan_run.argtypes = [P, P, P, P, P, P, P, C.POINTER(eik_stats)]
         L.eik_plan_destroy.argtypes = [P]
-        for f in ("eik_plan_gradient", "eik_plan_run", "eik_plan_destroy"):
+        L.eik_tracerays.argtypes = [P, C.POINTER(eik_grid), C.c_int64, P, P, P, P, C.c_double, P, P, C.c_int64,
+                                    C.POINTER(eik_stats)]
+        L.eik_traveltime_rays.argtypes = [P, C.c_int64, C.c_int64, P, P, P, C.POINTER(eik_extra), C.c_double, P,
+                                          P, P, C.c_int64, C.POINTER(eik_stats)]
+        for f in ("eik_plan_gradient", "eik_plan_run", "eik_plan_destroy", "eik_tracerays", "eik_traveltime_rays"):
             getattr(L, f).restype = C.c_int
         for f in ("eik_ctx_create", "eik_ctx_destroy", "eik_model_upload", "eik_model_upload_device",
                   "eik_model_release", "eik_traveltime", "eik_gradient", "eik_gradient_device"):

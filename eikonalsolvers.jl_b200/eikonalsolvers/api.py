@@ -71,6 +71,23 @@ class Context:
     def release(self, model: int):
         _lib.check(self.L.eik_model_release(self.h, C.c_int64(model)), self.h)
 
+    def traveltime_rays(self, model: int, grd, coordsrc, coordrec, steplen: float = 0.01, extraparams=None):
+        """Picks and rays in one device pipeline (the traveltime grids never leave the GPU):
+        returns (picks, rays) as ``traveltime`` and ``tracerays`` return them."""
+        cs, recoff, rec = _ray_inputs(grd, coordsrc, coordrec)
+        picks = np.zeros(max(int(recoff[-1]), 1), dtype=np.float64)
+        ep = _lib.extra_struct(extraparams)
+        st = _lib.eik_stats()
+
+        def call(npts, pts, cap):
+            return self.L.eik_traveltime_rays(self.h, C.c_int64(model), cs.shape[0], _lib.ptr(cs), _lib.ptr(recoff),
+                                              _lib.ptr(rec), C.byref(ep), float(steplen), _lib.ptr(picks),
+                                              _lib.ptr(npts), _lib.ptr(pts), cap, C.byref(st))
+        rc, rays = _traced(call, grd, cs, recoff, rec, steplen)
+        self.last_stats = st
+        _lib.check(rc, self.h)
+        return [picks[recoff[s]:recoff[s + 1]].copy() for s in range(cs.shape[0])], rays
+
     def plan_gradient(self, model: int, grd, coordsrc, coordrec, whichgrad, extraparams=None,
                       nthreads: int = 1) -> "GradientPlan":
         """Captures the gradient pipeline of this workload as a CUDA graph (GradientPlan)."""
@@ -224,6 +241,81 @@ class GradientPlan:
 
     def __exit__(self, *a):
         self.close()
+
+
+def _ray_inputs(grd, coordsrc, coordrec):
+    cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+    if isinstance(coordrec, np.ndarray) and coordrec.dtype != object:
+        coordrec = [coordrec]
+    recs = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+    assert cs.shape[0] == len(recs), "size(coordsrc,1)==length(coordrec)"
+    recoff = np.zeros(len(recs) + 1, dtype=np.int64)
+    for s, r in enumerate(recs):
+        recoff[s + 1] = recoff[s] + r.shape[0]
+    rec = np.ascontiguousarray(np.concatenate(recs, axis=0)) if recs else np.zeros((0, grd.ndim))
+    return cs, recoff, rec
+
+
+def _ray_capacity(grd, cs, recoff, rec, steplen) -> int:
+    """A generous first guess of the points of all rays (3x the straight-line distance)."""
+    rstep = steplen * grd.spacing[0] if grd.kind in (0, 1) else steplen
+    cap = 0
+    for s in range(cs.shape[0]):
+        for r in range(recoff[s], recoff[s + 1]):
+            if grd.kind in (0, 1):
+                d = float(np.linalg.norm(rec[r] - cs[s]))
+            else:  # polar coordinates, degrees
+                a, b = rec[r], cs[s]
+                d = float(np.sqrt(max(a[0] ** 2 + b[0] ** 2 - 2 * a[0] * b[0] * np.cos(np.deg2rad(a[1] - b[1])), 0)))
+            cap += int(3.0 * d / rstep) + 16
+    return cap
+
+
+def _split_rays(npts, pts, recoff, nd):
+    out, k = [], 0
+    for s in range(len(recoff) - 1):
+        rays = []
+        for r in range(recoff[s], recoff[s + 1]):
+            n = int(npts[r])
+            rays.append(pts[k * nd:(k + n) * nd].reshape(n, nd).copy())
+            k += n
+        out.append(rays)
+    return out
+
+
+def _traced(call, grd, cs, recoff, rec, steplen):
+    """Runs a ray-tracing entry point, again with the exact size when the first guess was short."""
+    npts = np.zeros(max(int(recoff[-1]), 1), dtype=np.int64)
+    cap = _ray_capacity(grd, cs, recoff, rec, steplen)
+    pts = np.zeros(cap * grd.ndim, dtype=np.float64)
+    rc = call(npts, pts, cap)
+    if rc == -5:  # EIK_ERR_OUT_OF_BUDGET: the rays are longer than the guess
+        cap = int(npts[:recoff[-1]].sum())
+        pts = np.zeros(cap * grd.ndim, dtype=np.float64)
+        rc = call(npts, pts, cap)
+    return rc, _split_rays(npts, pts, recoff, grd.ndim)
+
+
+def tracerays(grd, ttime, coordsrc, coordrec, steplen: float = 0.01, ctx: Optional[Context] = None):
+    """Rays from every receiver to its source through the traveltime grids ``ttime`` (one per
+    source, as ``eiktraveltime(...; returntt=true)`` returns them) (eikutils.jl:201-213).
+    Returns, per source, a list of (npoints, ndim) arrays, receiver first, source last."""
+    ctx = ctx or default_context()
+    cs, recoff, rec = _ray_inputs(grd, coordsrc, coordrec)
+    assert len(ttime) == cs.shape[0], "length(ttime)==size(coordsrc,1)"
+    for t in ttime:
+        assert tuple(np.shape(t)) == tuple(grd.grsize), "size(ttime[s])==grd.grsize"
+    tt = np.ascontiguousarray(np.concatenate([np.asarray(t, dtype=np.float64).ravel(order="F") for t in ttime]))
+    g = _lib.grid_struct(grd)
+    st = _lib.eik_stats()
+
+    def call(npts, pts, cap):
+        return ctx.L.eik_tracerays(ctx.h, C.byref(g), cs.shape[0], _lib.ptr(tt), _lib.ptr(cs), _lib.ptr(recoff),
+                                   _lib.ptr(rec), float(steplen), _lib.ptr(npts), _lib.ptr(pts), cap, C.byref(st))
+    rc, rays = _traced(call, grd, cs, recoff, rec, steplen)
+    ctx.last_stats = st
+    _lib.check(rc, ctx.h)
+    return rays
 
 
 _default: dict = {}

@@ -182,6 +182,24 @@ int eik_plan_run(eik_plan* plan, const double* vel, const double* pickobs, const
                  double* gradvel, double* gradsrc, double* misfit, eik_stats* stats);
 int eik_plan_destroy(eik_plan* plan);
 
+/* Replaces tracerays (eikutils.jl:201-328): for every receiver of every source the ray from
+ * the receiver to the source, following the cubic B-spline gradient of the source's
+ * traveltime grid in steps of steplen*h (steplen on Grid2DSphere); Grid3DSphere errors as in
+ * the reference. ttgrids: host, nsrc x N column-major grids (as eik_traveltime returns them).
+ * ray_npts (out): rec_off[nsrc] point counts. paths (nullable): room for paths_cap points of
+ * ndim doubles; the rays are written there, concatenated in receiver order, when they fit,
+ * else EIK_ERR_OUT_OF_BUDGET is returned with ray_npts filled (call again with a larger
+ * buffer). A ray that needs more than 2^24 steps fails with EIK_ERR_NOT_CONVERGED. */
+int eik_tracerays(eik_ctx* ctx, const eik_grid* grd, int64_t nsrc, const double* ttgrids,
+                  const double* coordsrc, const int64_t* rec_off, const double* rec, double steplen,
+                  int64_t* ray_npts, double* paths, int64_t paths_cap, eik_stats* stats);
+/* Traveltimes (picks as eik_traveltime) and rays in one device pipeline: the traveltime
+ * grids stay in device memory between the solve and the ray tracing. */
+int eik_traveltime_rays(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
+                        const int64_t* rec_off, const double* rec, const eik_extra* ep, double steplen,
+                        double* picks, int64_t* ray_npts, double* paths, int64_t paths_cap,
+                        eik_stats* stats);
+
 /* No counterpart in the reference. Misfit 0.5*Σ_s Σ_r (t - obs)²/σ² of nsrc traveltime
  * grids that are already in device memory (ttgrids_dev: nsrc x N, as eik_traveltime
  * returns them), with receivers, observations and the result also in device memory and

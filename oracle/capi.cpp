@@ -165,4 +165,30 @@ int eikor_smoothgradient(int kind, const int64_t* grsize, const double* spacing,
   }
 }
 
+// Rays: pass 1 (pts NULL or cap too small) returns the point counts in npts and the total
+// in *total; pass 2 with cap >= total also writes the points.
+int eikor_tracerays(int kind, const int64_t* grsize, const double* spacing, const double* cooinit,
+                    const double* ttgrids, int64_t nsrc, const double* coordsrc, const int64_t* recoff,
+                    const double* rec, double steplen, int64_t max_steps, int64_t* npts, double* pts,
+                    int64_t cap, int64_t* total, char* errbuf, int errlen) {
+  try {
+    Grid g = make_grid(kind, grsize, spacing, cooinit);
+    std::vector<i64> np;
+    std::vector<double> pp;
+    tracerays(g, ttgrids, nsrc, coordsrc, recoff, rec, steplen, max_steps, np, pp);
+    i64 tot = 0;
+    for (size_t r = 0; r < np.size(); r++) {
+      npts[r] = np[r];
+      tot += np[r];
+    }
+    *total = tot;
+    if (pts && cap >= tot) std::memcpy(pts, pp.data(), sizeof(double) * pp.size());
+    return 0;
+  } catch (const OracleError& e) {
+    return report(e, errbuf, errlen, e.code);
+  } catch (const std::exception& e) {
+    return report(e, errbuf, errlen, 3);
+  }
+}
+
 }  // extern "C"

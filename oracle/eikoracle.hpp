@@ -202,4 +202,9 @@ void eikgradient(const Grid& g, const double* vel, i64 nsrc, const double* coord
 void smoothgradaroundsrc(std::vector<double>& grad, const double* xyzsrc, const Grid& g, i64 radiuspx);
 void smoothgradient(i64 l, const Grid& g, std::vector<double>& grad);
 
+// tracerays (eikutils.jl:201-328), oracle/rays.cpp. npts per receiver (recoff order),
+// points concatenated row-major.
+void tracerays(const Grid& g, const double* ttgrids, i64 nsrc, const double* coordsrc, const i64* recoff,
+               const double* rec, double steplen, i64 max_steps, std::vector<i64>& npts, std::vector<double>& pts);
+
 }  // namespace eikor

@@ -47,7 +47,7 @@ def lib():
     global _LIB
     if _LIB is None:
         path = os.path.join(_HERE, "libeikoracle.so")
-        srcs = [os.path.join(_HERE, f) for f in ("fwd.cpp", "grad.cpp", "capi.cpp", "eikoracle.hpp")]
+        srcs = [os.path.join(_HERE, f) for f in ("fwd.cpp", "grad.cpp", "rays.cpp", "capi.cpp", "eikoracle.hpp")]
         if not os.path.exists(path) or any(os.path.getmtime(s) > os.path.getmtime(path) for s in srcs if os.path.exists(s)):
             build()
         L = C.CDLL(path)
@@ -67,6 +67,9 @@ def lib():
         L.eikor_range_value.restype = C.c_double
         L.eikor_smoothgradient.argtypes = [C.c_int, P, P, P, C.c_int64, P, C.c_char_p, C.c_int]
         L.eikor_smoothgradient.restype = C.c_int
+        L.eikor_tracerays.argtypes = [C.c_int, P, P, P, P, C.c_int64, P, P, P, C.c_double, C.c_int64, P, P,
+                                      C.c_int64, P, C.c_char_p, C.c_int]
+        L.eikor_tracerays.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -239,3 +242,36 @@ def smoothgradient(l: int, grd, grad) -> np.ndarray:
     buf = C.create_string_buffer(512)
     _check(L.eikor_smoothgradient(grd.kind, _p(gs), _p(sp), _p(co), int(l), _p(g), buf, 512), buf)
     return g.reshape(grd.grsize, order="F")
+
+
+def tracerays(grd, ttime, coordsrc, coordrec, steplen: float = 0.01, max_steps: int = 1 << 26):
+    """Oracle of ``tracerays`` (eikutils.jl:201-328): per source, per receiver, the ray as an
+    (npoints, ndim) array from the receiver to the source."""
+    L = lib()
+    cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+    nsrc = cs.shape[0]
+    recs = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+    recoff = np.zeros(nsrc + 1, dtype=np.int64)
+    for i, r in enumerate(recs):
+        recoff[i + 1] = recoff[i] + r.shape[0]
+    rec = np.ascontiguousarray(np.concatenate(recs))
+    tt = np.ascontiguousarray(np.concatenate([np.asarray(t, dtype=np.float64).ravel(order="F") for t in ttime]))
+    gs, sp, co = _grid_arrays(grd)
+    npts = np.zeros(int(recoff[-1]), dtype=np.int64)
+    total = np.zeros(1, dtype=np.int64)
+    buf = C.create_string_buffer(512)
+    _check(L.eikor_tracerays(grd.kind, _p(gs), _p(sp), _p(co), _p(tt), nsrc, _p(cs), _p(recoff), _p(rec),
+                             float(steplen), int(max_steps), _p(npts), None, 0, _p(total), buf, 512), buf)
+    pts = np.zeros(int(total[0]) * grd.ndim, dtype=np.float64)
+    _check(L.eikor_tracerays(grd.kind, _p(gs), _p(sp), _p(co), _p(tt), nsrc, _p(cs), _p(recoff), _p(rec),
+                             float(steplen), int(max_steps), _p(npts), _p(pts), int(total[0]), _p(total), buf,
+                             512), buf)
+    out, k = [], 0
+    for s in range(nsrc):
+        rays = []
+        for r in range(recoff[s], recoff[s + 1]):
+            n = int(npts[r])
+            rays.append(pts[k * grd.ndim:(k + n) * grd.ndim].reshape(n, grd.ndim).copy())
+            k += n
+        out.append(rays)
+    return out
