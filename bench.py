@@ -19,6 +19,8 @@ Lines printed by rank 0 (one JSON object):
   plain     the same workload one source per call (the unbatched path)
   roofline  HBM roofline of the dominant kernel (algorithmic bytes / measured duration)
   cpu_baseline  the oracle (C++ restatement of the reference algorithm) on the host cores
+  serve     the serving leg: Poisson arrivals of a mixed traveltime/gradient workload
+  rays      the ray-tracing leg (tracerays on 128^3 grids): GPU rays/s beside the oracle's
 
 --impl reference: times the oracle on the host cores instead (rank 0 only).
 """
@@ -61,6 +63,8 @@ def parse():
                     help="requests of the serving leg (Poisson arrivals; 0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=2.0, help="arrival rate of the serving leg, req/s")
     ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--ray-sources", type=int, default=8, help="sources of the ray-tracing leg (0 = skip)")
+    ap.add_argument("--ray-cpu-rays", type=int, default=24, help="rays the oracle traces for the CPU figure")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="grid scale of the serving mix")
     return ap.parse_args()
 
@@ -438,10 +442,55 @@ def main_b200(args):
                 line["serve"] = run_serve_leg(args, local)
             except Exception as e:
                 line["serve"] = {"error": str(e)}
+        if ws == 1 and args.ray_sources > 0:
+            try:
+                line["rays"] = run_rays_leg(args, local)
+            except Exception as e:
+                line["rays"] = {"error": str(e)}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
     return 0
+
+
+def run_rays_leg(args, device):
+    """Ray tracing (tracerays) on the 3D layered workload at 128^3: every receiver of
+    `ray_sources` sources, steplen 0.01 (the reference's default). GPU rays/s through
+    eik_tracerays with the traveltime grids and the rays in host memory (copies timed), beside
+    the oracle on the host cores for a sample of the same rays."""
+    from eikonalsolvers import Context, ExtraParams, tracerays
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import eikoracle as O
+    w = make_workload(0.5, args.ray_sources)
+    ctx = Context(device)
+    try:
+        mid = ctx.upload(w.vel, w.grd)
+        _, tt = ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec, returntt=True, extraparams=ExtraParams())
+        ctx.release(mid)
+        tracerays(w.grd, tt, w.coordsrc, w.coordrec, steplen=0.01, ctx=ctx)  # warm-up (scratch growth)
+        ms = []
+        for _ in range(3):
+            rays = tracerays(w.grd, tt, w.coordsrc, w.coordrec, steplen=0.01, ctx=ctx)
+            ms.append(float(ctx.last_stats.device_ms))
+    finally:
+        ctx.close()
+    nray = sum(len(r) for r in rays)
+    npts = sum(x.shape[0] for r in rays for x in r)
+    gpu_ms = min(ms)
+    # oracle: one source's spline and its first rays, single thread
+    k = max(1, min(args.ray_cpu_rays, len(w.coordrec[0])))
+    t0 = time.perf_counter()
+    ora = O.tracerays(w.grd, tt[:1], w.coordsrc[:1], [w.coordrec[0][:k]], steplen=0.01)
+    cpu_s = time.perf_counter() - t0
+    cpu_pts = sum(x.shape[0] for x in ora[0])
+    same = all(np.array_equal(a, b) for a, b in zip(ora[0], rays[0][:k]))
+    return {"workload": f"3D layered 128^3, {args.ray_sources} sources x 400 receivers, steplen 0.01",
+            "rays": nray, "points": npts, "gpu_ms": gpu_ms, "rays_per_s": nray / (gpu_ms / 1000.0),
+            "points_per_s": npts / (gpu_ms / 1000.0),
+            "gpu_timing": "eik_tracerays device time incl. the grids' upload and the paths' download, best of 3",
+            "cpu_baseline": {"rays_per_s": k / cpu_s, "points_per_s": cpu_pts / cpu_s, "cores": 1, "kind": "port",
+                             "sample": f"{k} rays of source 0 (spline of that source included)"},
+            "bit_identical_to_oracle_on_sample": bool(same)}
 
 
 def run_serve_leg(args, device):

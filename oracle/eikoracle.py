@@ -244,7 +244,7 @@ def smoothgradient(l: int, grd, grad) -> np.ndarray:
     return g.reshape(grd.grsize, order="F")
 
 
-def tracerays(grd, ttime, coordsrc, coordrec, steplen: float = 0.01, max_steps: int = 1 << 26):
+def tracerays(grd, ttime, coordsrc, coordrec, steplen: float = 0.01, max_steps: int = 1 << 24):
     """Oracle of ``tracerays`` (eikutils.jl:201-328): per source, per receiver, the ray as an
     (npoints, ndim) array from the receiver to the source."""
     L = lib()
