@@ -532,6 +532,11 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
     ctx->ctas_per_sm = (int)value;
     return EIK_OK;
   }
+  if (std::strcmp(name, "ray_room") == 0) {
+    if (!(value >= 0.0 && value <= 100.0)) return fail(ctx, EIK_ERR_ASSERT, "ray_room must be in [0, 100]");
+    ctx->ray_room = value;
+    return EIK_OK;
+  }
   if (std::strcmp(name, "fwd_queue") == 0) {
     if (!(value == -1.0 || value == 0.0 || value == 1.0))
       return fail(ctx, EIK_ERR_ASSERT, "fwd_queue must be -1 (automatic), 0 or 1");

@@ -12,9 +12,11 @@
 // operation for operation, so Cartesian rays are bit-identical to it (the spherical step
 // also calls sin, cos and atan2).
 //
-// Tracing: one thread per ray, twice: the first pass counts the points of every ray, the
-// host turns the counts into offsets, the second pass recomputes the rays and writes them.
-// A ray longer than the step limit sets an error bit and stops.
+// Tracing: one thread per ray, in one pass that writes every ray into a room of three times
+// its straight-line length plus 16 points and counts its points; a compaction kernel then
+// moves the rays to their places in the output (the rare ray that outgrows its room makes the
+// pass run again, each ray with exactly its room). A ray longer than the step limit sets an
+// error bit and stops.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -43,6 +45,17 @@ __global__ void spline_axis_kernel(SplineArgs s, int ax, const double* cp) {
     spline_line(s, ax, cp, q);
 }
 
+// Rays from their rooms in the slab to their places in the output, one block per ray.
+__global__ void ray_compact_kernel(const double* slab, const long long* soff, const long long* npts,
+                                   const long long* outoff, double* out, long long nray, int nd) {
+  for (long long r = blockIdx.x; r < nray; r += gridDim.x) {
+    const long long n = npts[r] * nd;
+    const double* src = slab + soff[r] * nd;
+    double* dst = out + outoff[r] * nd;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  }
+}
+
 template <int ND>
 __global__ void __launch_bounds__(RAY_THREADS) trace_kernel(RayArgs a, int write) {
   const long long nray = a.recoff[a.nsrc];
@@ -63,8 +76,9 @@ static std::vector<double> thomas_factors(long long k) {
 // other inputs are on the device too except rec_off (host). ray_npts (host) receives the
 // point counts; paths (host, nullable) the points when paths_cap is large enough.
 int trace_device(eik_ctx* ctx, const GridDesc& g, int64_t nsrc, const double* d_tt, const double* d_cs,
-                 const long long* d_off, const double* d_rec, const int64_t* rec_off, double steplen,
-                 int64_t* ray_npts, double* paths, int64_t paths_cap, eik_stats* stats) {
+                 const long long* d_off, const double* d_rec, const double* h_cs, const int64_t* rec_off,
+                 const double* h_rec, double steplen, int64_t* ray_npts, double* paths, int64_t paths_cap,
+                 eik_stats* stats) {
   int rc = EIK_OK;
   cudaStream_t st = ctx->stream;
   Scratch& S = ctx->scratch;
@@ -126,48 +140,101 @@ int trace_device(eik_ctx* ctx, const GridDesc& g, int64_t nsrc, const double* d_
   ra.thrdist = g.spac[0] * sqrt(2.0);
   ra.max_steps = 1LL << 24;
   ra.outoff = d_oo;
+  ra.cap = nullptr;
   ra.npts = d_np;
   ra.pts = nullptr;
   ra.err = d_err;
   const int nblk = (int)std::max<long long>(1, std::min<long long>((nray + RAY_THREADS - 1) / RAY_THREADS, 1 << 16));
-  if (nray) {
-    if (g.nd == 3) trace_kernel<3><<<nblk, RAY_THREADS, 0, st>>>(ra, 0);
-    else trace_kernel<2><<<nblk, RAY_THREADS, 0, st>>>(ra, 0);
-  }
-  CUDA_OK(ctx, cudaGetLastError());
+  int launches = 0;
+  auto launch = [&](int write) {
+    if (!nray) return;
+    if (g.nd == 3) trace_kernel<3><<<nblk, RAY_THREADS, 0, st>>>(ra, write);
+    else trace_kernel<2><<<nblk, RAY_THREADS, 0, st>>>(ra, write);
+    launches++;
+  };
   std::vector<long long> cnt((size_t)std::max<long long>(nray, 1), 0);
-  uint32_t herr = 0;
-  if (nray) CUDA_OK(ctx, cudaMemcpyAsync(cnt.data(), d_np, sizeof(long long) * nray, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(ctx, cudaMemcpyAsync(&herr, d_err, sizeof herr, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(ctx, cudaStreamSynchronize(st));
-  if (herr & ERRB_RAY_ADDR) return fail(ctx, EIK_ERR_ERROR, "ray kernels: an address check failed (0x%x)", herr);
-  if (herr & ERRB_RAY_STEPS) return fail(ctx, EIK_ERR_NOT_CONVERGED, "a ray did not reach its source within 2^24 steps");
+  auto read_counts = [&]() -> int {
+    uint32_t herr = 0;
+    CUDA_OK(ctx, cudaGetLastError());
+    if (nray) CUDA_OK(ctx, cudaMemcpyAsync(cnt.data(), d_np, sizeof(long long) * nray, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(ctx, cudaMemcpyAsync(&herr, d_err, sizeof herr, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(ctx, cudaStreamSynchronize(st));
+    if (herr & ERRB_RAY_ADDR) return fail(ctx, EIK_ERR_ERROR, "ray kernels: an address check failed (0x%x)", herr);
+    if (herr & ERRB_RAY_STEPS)
+      return fail(ctx, EIK_ERR_NOT_CONVERGED, "a ray did not reach its source within 2^24 steps");
+    return EIK_OK;
+  };
+  if (!paths) {  // counts only
+    launch(0);
+    rc = read_counts();
+    if (rc) return rc;
+    for (long long r = 0; r < nray; r++) ray_npts[r] = cnt[(size_t)r];
+    if (stats) stats->launches += 1 + g.nd + launches;
+    return EIK_OK;
+  }
+  // one pass that writes every ray into a room of ray_room (3) times its straight-line length
+  // (in steps) plus 16 points; the rays that outgrow their room are traced again below
+  std::vector<long long> room((size_t)std::max<long long>(nray, 1)), soff((size_t)std::max<long long>(nray, 1));
+  long long slab = 0;
+  for (int64_t s = 0; s < nsrc; s++)
+    for (long long r = rec_off[s]; r < rec_off[s + 1]; r++) {
+      const double dist = distance2points(g, h_rec + r * g.nd, h_cs + s * g.nd);
+      const double est = std::isfinite(dist) ? ctx->ray_room * dist / ra.rstep : 0.0;
+      room[(size_t)r] = (est < 1e7 ? (long long)est : 10000000LL) + 16;
+      soff[(size_t)r] = slab;
+      slab += room[(size_t)r];
+    }
+  long long* d_room;
+  double* d_slab;
+  GET(d_room, long long, "ray_room", std::max<long long>(nray, 1));
+  GET(d_slab, double, "ray_slab", std::max<long long>(slab, 1) * g.nd);
+  if (nray) {
+    CUDA_OK(ctx, cudaMemcpyAsync(d_room, room.data(), sizeof(long long) * nray, cudaMemcpyHostToDevice, st));
+    CUDA_OK(ctx, cudaMemcpyAsync(d_oo, soff.data(), sizeof(long long) * nray, cudaMemcpyHostToDevice, st));
+  }
+  ra.cap = d_room;
+  ra.pts = d_slab;
+  ra.pts_size = slab * g.nd;
+  launch(1);
+  rc = read_counts();
+  if (rc) return rc;
   std::vector<long long> off((size_t)std::max<long long>(nray, 1), 0);
   long long total = 0;
+  bool outgrown = false;
   for (long long r = 0; r < nray; r++) {
     ray_npts[r] = cnt[(size_t)r];
     off[(size_t)r] = total;
     total += cnt[(size_t)r];
+    outgrown = outgrown || cnt[(size_t)r] > room[(size_t)r];
   }
-  if (stats) stats->launches += 2 + g.nd;
-  if (!paths) return EIK_OK;
   if (total > paths_cap)
     return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "the rays have %lld points, paths has room for %lld", total,
                 (long long)paths_cap);
   double* d_pts;
+  long long* d_xoff;
   GET(d_pts, double, "ray_pts", std::max<long long>(total, 1) * g.nd);
+  GET(d_xoff, long long, "ray_xoff", std::max<long long>(nray, 1));
 #undef GET
-  CUDA_OK(ctx, cudaMemcpyAsync(d_oo, off.data(), sizeof(long long) * nray, cudaMemcpyHostToDevice, st));
-  ra.pts = d_pts;
-  ra.pts_size = total * g.nd;
-  if (g.nd == 3) trace_kernel<3><<<nblk, RAY_THREADS, 0, st>>>(ra, 1);
-  else trace_kernel<2><<<nblk, RAY_THREADS, 0, st>>>(ra, 1);
+  if (nray) CUDA_OK(ctx, cudaMemcpyAsync(d_xoff, off.data(), sizeof(long long) * nray, cudaMemcpyHostToDevice, st));
+  if (!outgrown) {
+    ray_compact_kernel<<<(int)std::min<long long>(std::max<long long>(nray, 1), 1 << 16), 128, 0, st>>>(
+        d_slab, d_oo, d_np, d_xoff, d_pts, nray, g.nd);
+    launches++;
+  } else {  // trace every ray again, each with exactly its room
+    if (nray) {
+      CUDA_OK(ctx, cudaMemcpyAsync(d_room, cnt.data(), sizeof(long long) * nray, cudaMemcpyHostToDevice, st));
+      CUDA_OK(ctx, cudaMemcpyAsync(d_oo, off.data(), sizeof(long long) * nray, cudaMemcpyHostToDevice, st));
+    }
+    ra.pts = d_pts;
+    ra.pts_size = total * g.nd;
+    launch(1);
+    rc = read_counts();
+    if (rc) return rc;
+  }
   CUDA_OK(ctx, cudaGetLastError());
   CUDA_OK(ctx, cudaMemcpyAsync(paths, d_pts, sizeof(double) * total * g.nd, cudaMemcpyDeviceToHost, st));
-  CUDA_OK(ctx, cudaMemcpyAsync(&herr, d_err, sizeof herr, cudaMemcpyDeviceToHost, st));
   CUDA_OK(ctx, cudaStreamSynchronize(st));
-  if (herr & ERRB_RAY_ADDR) return fail(ctx, EIK_ERR_ERROR, "ray kernels: an address check failed (0x%x)", herr);
-  if (stats) stats->launches += 1;
+  if (stats) stats->launches += 1 + g.nd + launches;
   return EIK_OK;
 }
 
@@ -218,7 +285,7 @@ extern "C" int eik_tracerays(eik_ctx* ctx, const eik_grid* grd, int64_t nsrc, co
   CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * g.nd, cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
   if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * g.nd, cudaMemcpyHostToDevice, st));
-  rc = trace_device(ctx, g, nsrc, d_tt, d_cs, d_off, d_rec, rec_off, steplen, ray_npts, paths, paths_cap, stats);
+  rc = trace_device(ctx, g, nsrc, d_tt, d_cs, d_off, d_rec, coordsrc, rec_off, rec, steplen, ray_npts, paths, paths_cap, stats);
   cudaEventRecord(ctx->ev1, st);
   cudaStreamSynchronize(st);
   if (stats) {
@@ -273,7 +340,7 @@ extern "C" int eik_traveltime_rays(eik_ctx* ctx, eik_model_id model, int64_t nsr
   rc = collect_forward_stats(ctx, &fw, stats);
   if (rc) return rc;
   // the traveltime grids never leave the device
-  rc = trace_device(ctx, m.g, nsrc, fw.t, d_cs, d_off, d_rec, rec_off, steplen, ray_npts, paths, paths_cap, stats);
+  rc = trace_device(ctx, m.g, nsrc, fw.t, d_cs, d_off, d_rec, coordsrc, rec_off, rec, steplen, ray_npts, paths, paths_cap, stats);
   cudaEventRecord(ctx->ev1, st);
   cudaStreamSynchronize(st);
   if (stats) {

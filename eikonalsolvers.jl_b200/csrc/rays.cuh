@@ -117,8 +117,9 @@ struct RayArgs {
   const double* rec;
   double rstep, thrdist;
   long long max_steps;
-  const long long* outoff;  // second pass: first point of every ray
-  long long* npts;          // first pass: points of every ray
+  const long long* outoff;  // writing: first point of every ray
+  const long long* cap;     // writing: room (points) of every ray at outoff
+  long long* npts;          // points of every ray
   double* pts;
   uint32_t* err;
 };
@@ -147,34 +148,44 @@ EIK_HD bool spline_gradient(const RayArgs& a, const double* c, const double* x, 
     ix[d] = i;
     bweights(u - (double)i, w[d], dw[d]);
   }
-  for (int gd = 0; gd < ND; gd++) {
-    double acc = 0.0;
-    if (ND == 2) {
-      for (int bb = 0; bb < 4; bb++) {
-        const double wb = (gd == 1) ? dw[1][bb] : w[1][bb];
-        const double* crow = c + (ix[0] - 1) + a.m[0] * (ix[1] - 1 + bb);
-        if (!ray_span_ok<double>(crow, 4, a.coef, a.coef_size)) return false;
-        double row = 0.0;
-        for (int aa = 0; aa < 4; aa++) row = row + ((gd == 0) ? dw[0][aa] : w[0][aa]) * RAY_LD(crow + aa);
-        acc = acc + wb * row;
+  // every coefficient is loaded once; each gradient component keeps its own row / plane /
+  // total sums, accumulated in the same order as a component-by-component evaluation
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (ND == 2) {
+    for (int bb = 0; bb < 4; bb++) {
+      const double* crow = c + (ix[0] - 1) + a.m[0] * (ix[1] - 1 + bb);
+      if (!ray_span_ok<double>(crow, 4, a.coef, a.coef_size)) return false;
+      double row[2] = {0.0, 0.0};
+      for (int aa = 0; aa < 4; aa++) {
+        const double cv = RAY_LD(crow + aa);
+        row[0] = row[0] + dw[0][aa] * cv;
+        row[1] = row[1] + w[0][aa] * cv;
       }
-    } else {
-      for (int cc = 0; cc < 4; cc++) {
-        const double wc = (gd == 2) ? dw[2][cc] : w[2][cc];
-        double plane = 0.0;
-        for (int bb = 0; bb < 4; bb++) {
-          const double wb = (gd == 1) ? dw[1][bb] : w[1][bb];
-          const double* crow = c + (ix[0] - 1) + a.m[0] * ((ix[1] - 1 + bb) + a.m[1] * (ix[2] - 1 + cc));
-          if (!ray_span_ok<double>(crow, 4, a.coef, a.coef_size)) return false;
-          double row = 0.0;
-          for (int aa = 0; aa < 4; aa++) row = row + ((gd == 0) ? dw[0][aa] : w[0][aa]) * RAY_LD(crow + aa);
-          plane = plane + wb * row;
-        }
-        acc = acc + wc * plane;
-      }
+      acc[0] = acc[0] + w[1][bb] * row[0];
+      acc[1] = acc[1] + dw[1][bb] * row[1];
     }
-    grad[gd] = acc / a.g.spac[gd];
+  } else {
+    for (int cc = 0; cc < 4; cc++) {
+      double plane[3] = {0.0, 0.0, 0.0};
+      for (int bb = 0; bb < 4; bb++) {
+        const double* crow = c + (ix[0] - 1) + a.m[0] * ((ix[1] - 1 + bb) + a.m[1] * (ix[2] - 1 + cc));
+        if (!ray_span_ok<double>(crow, 4, a.coef, a.coef_size)) return false;
+        double rd = 0.0, rw = 0.0;  // rows with the derivative / value weights along x
+        for (int aa = 0; aa < 4; aa++) {
+          const double cv = RAY_LD(crow + aa);
+          rd = rd + dw[0][aa] * cv;
+          rw = rw + w[0][aa] * cv;
+        }
+        plane[0] = plane[0] + w[1][bb] * rd;
+        plane[1] = plane[1] + dw[1][bb] * rw;
+        plane[2] = plane[2] + w[1][bb] * rw;
+      }
+      acc[0] = acc[0] + w[2][cc] * plane[0];
+      acc[1] = acc[1] + w[2][cc] * plane[1];
+      acc[2] = acc[2] + dw[2][cc] * plane[2];
+    }
   }
+  for (int gd = 0; gd < ND; gd++) grad[gd] = acc[gd] / a.g.spac[gd];
   return true;
 }
 
@@ -211,7 +222,9 @@ EIK_HD bool ray_step(const RayArgs& a, const double* c, const double* pt, double
   return true;
 }
 
-// Ray r: counts its points (write = 0) or writes them at outoff[r] (write = 1).
+// Ray r: counts its points into npts[r] and, when write is set, writes those that fit in
+// its room cap[r] at outoff[r] (a ray longer than its room is counted in full; the caller
+// traces it again with enough room).
 template <int ND>
 EIK_HD void trace_one(const RayArgs& a, long long r, int write) {
   int s = 0;
@@ -225,9 +238,10 @@ EIK_HD void trace_one(const RayArgs& a, long long r, int write) {
   double pt[3] = {0.0, 0.0, 0.0}, nw[3] = {0.0, 0.0, 0.0};
   for (int d = 0; d < ND; d++) pt[d] = a.rec[r * ND + d];
   double* out = nullptr;
-  if (write) {
+  const long long room = write ? a.cap[r] : 0;
+  if (write && room > 0) {
     out = a.pts + a.outoff[r] * ND;
-    if (!ray_span_ok<double>(out, ND, a.pts, a.pts_size)) {
+    if (!ray_span_ok<double>(out, room * ND, a.pts, a.pts_size)) {
       RAY_OR(a.err, ERRB_RAY_ADDR);
       return;
     }
@@ -240,22 +254,21 @@ EIK_HD void trace_one(const RayArgs& a, long long r, int write) {
       RAY_OR(a.err, ERRB_RAY_STEPS);
       break;
     }
-    if (!ray_step<ND>(a, c, pt, nw) || (write && !ray_span_ok<double>(out + np * ND, ND, a.pts, a.pts_size))) {
+    if (!ray_step<ND>(a, c, pt, nw)) {
       RAY_OR(a.err, ERRB_RAY_ADDR);
       return;
     }
     for (int d = 0; d < ND; d++) {
       pt[d] = nw[d];
-      if (write) out[np * ND + d] = nw[d];
+      if (np < room) out[np * ND + d] = nw[d];
     }
     dist = distance2points(a.g, pt, src);
     np++;
   }
-  if (write) {  // the last point is the source (eikutils.jl:319)
+  if (np <= room) {  // the last point is the source (eikutils.jl:319)
     for (int d = 0; d < ND; d++) out[(np - 1) * ND + d] = src[d];
-  } else {
-    a.npts[r] = np;
   }
+  a.npts[r] = np;
 }
 
 }  // namespace eik

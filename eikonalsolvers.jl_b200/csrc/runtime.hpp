@@ -104,6 +104,7 @@ struct eik_ctx {
   int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
   int fwd_queue = -1;        // per-warp evaluation queue of the forward solve: -1 by size, 0 off, 1 on
   double sm_fraction = 1.0; // share of the SMs the persistent (cooperative) solves of this context use
+  double ray_room = 3.0;     // room of a ray in its first tracing pass, in straight-line lengths
   bool fine_replay = false; // refined start-up by exact heap replay for every source (else only on ties)
   int solve_sms() const {
     const int n = (int)(sm_fraction * (double)nsm + 0.5);

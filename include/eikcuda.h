@@ -127,7 +127,9 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * together); "ctas_per_sm" = resident CTAs per SM of the forward solve, an integer, 0 (the
  * default) = as many as fit; "fwd_queue" = how the forward solve's warps work through their
  * entries: 1 = evaluations queued per warp and run 32 at a time, 0 = each in place, -1 (the
- * default) = the queue from 2^27 node-sources per launch up; "fine_replay" = 1 replays the refined start-up's heap for every
+ * default) = the queue from 2^27 node-sources per launch up; "ray_room" = room of a ray in
+ * the single tracing pass, in multiples of its straight-line length (default 3; rays that
+ * outgrow it are traced again); "fine_replay" = 1 replays the refined start-up's heap for every
  * source instead of only where an exact tie decides its stop (default 0). Returns
  * EIK_ERR_ASSERT for an unknown name or a value out of range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);

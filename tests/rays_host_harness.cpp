@@ -43,8 +43,16 @@ int main(int argc, char** argv) {
   std::vector<long long> np(nray), oo(nray); uint32_t err = 0; ra.npts = np.data(); ra.outoff = oo.data(); ra.err = &err;
   for (long long r = 0; r < nray; r++) { if (g.nd == 3) trace_one<3>(ra, r, 0); else trace_one<2>(ra, r, 0); }
   long long tot = 0; for (long long r = 0; r < nray; r++) { oo[r] = tot; tot += np[r]; }
-  std::vector<double> pts(tot * g.nd); ra.pts = pts.data(); ra.pts_size = tot * g.nd;
+  // writing pass with a room of exactly the counted points for odd rays and a generous one
+  // (the counted points plus 7) for even rays, in the layout of a slab
+  std::vector<long long> room(nray), soff(nray); long long slab = 0;
+  for (long long r = 0; r < nray; r++) { room[r] = np[r] + ((r % 2) ? 0 : 7); soff[r] = slab; slab += room[r]; }
+  std::vector<double> sl(slab * g.nd); ra.pts = sl.data(); ra.pts_size = slab * g.nd; ra.cap = room.data(); ra.outoff = soff.data();
+  std::vector<long long> np2(nray); ra.npts = np2.data();
   for (long long r = 0; r < nray; r++) { if (g.nd == 3) trace_one<3>(ra, r, 1); else trace_one<2>(ra, r, 1); }
+  for (long long r = 0; r < nray; r++) if (np2[r] != np[r]) { printf("count mismatch\n"); return 3; }
+  std::vector<double> pts(tot * g.nd);
+  for (long long r = 0; r < nray; r++) std::memcpy(pts.data() + oo[r] * g.nd, sl.data() + soff[r] * g.nd, sizeof(double) * np[r] * g.nd);
   FILE* o = fopen(argv[6], "wb"); fwrite(np.data(), 8, nray, o); fwrite(pts.data(), 8, pts.size(), o); fclose(o);
   printf("rays %lld points %lld err %u spline_err %u\n", nray, tot, err, serr);
   return 0;

@@ -83,3 +83,18 @@ def test_ray_errors(ctx):
     with pytest.raises(RuntimeError, match="not yet implemented"):
         tracerays(g3, [np.ones(g3.grsize)], np.array([[5806.0, 41.0, 11.0]]), [np.array([[5810.0, 41.5, 11.5]])],
                   ctx=ctx)
+
+
+def test_rays_that_outgrow_their_room_are_traced_again(ctx):
+    """ray_room 0 gives every ray a room of 16 points in the single pass, so the long ones take
+    the second pass: same rays as with the default room."""
+    w = CF.cfg3(scale=0.125, nsrc=2, nrec_side=3)
+    _, tt = O.eiktraveltime(w.vel, w.grd, w.coordsrc, w.coordrec, returntt=True)
+    want = tracerays(w.grd, tt, w.coordsrc, w.coordrec, steplen=0.02, ctx=ctx)
+    ctx.set_param("ray_room", 0.0)
+    try:
+        got = tracerays(w.grd, tt, w.coordsrc, w.coordrec, steplen=0.02, ctx=ctx)
+    finally:
+        ctx.set_param("ray_room", 3.0)
+    for a, b in zip(got, want):
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
