@@ -21,6 +21,7 @@ Lines printed by rank 0 (one JSON object):
   cpu_baseline  the oracle (C++ restatement of the reference algorithm) on the host cores
   serve     the serving leg: Poisson arrivals of a mixed traveltime/gradient workload
   rays      the ray-tracing leg (tracerays on 128^3 grids): GPU rays/s beside the oracle's
+  hmc       HMC-style evaluations: eik_gradient per new velocity vs a replayed CUDA-graph plan
 
 --impl reference: times the oracle on the host cores instead (rank 0 only).
 """
@@ -64,6 +65,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=2.0, help="arrival rate of the serving leg, req/s")
     ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--ray-sources", type=int, default=8, help="sources of the ray-tracing leg (0 = skip)")
+    ap.add_argument("--hmc-evals", type=int, default=20, help="evaluations of the HMC-style leg (0 = skip)")
     ap.add_argument("--ray-cpu-rays", type=int, default=24, help="rays the oracle traces for the CPU figure")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="grid scale of the serving mix")
     return ap.parse_args()
@@ -442,6 +444,11 @@ def main_b200(args):
                 line["serve"] = run_serve_leg(args, local)
             except Exception as e:
                 line["serve"] = {"error": str(e)}
+        if ws == 1 and args.hmc_evals > 0:
+            try:
+                line["hmc"] = run_hmc_leg(args, local)
+            except Exception as e:
+                line["hmc"] = {"error": str(e)}
         if ws == 1 and args.ray_sources > 0:
             try:
                 line["rays"] = run_rays_leg(args, local)
@@ -491,6 +498,53 @@ def run_rays_leg(args, device):
             "cpu_baseline": {"rays_per_s": k / cpu_s, "points_per_s": cpu_pts / cpu_s, "cores": 1, "kind": "port",
                              "sample": f"{k} rays of source 0 (spline of that source included)"},
             "bit_identical_to_oracle_on_sample": bool(same)}
+
+
+def run_hmc_leg(args, device):
+    """HMC-style evaluations (the pattern of HMCtraveltimes.jl: eikgradient model after model
+    with the same sources and receivers) on the 2D Cartesian 300x220 grid of the reference's
+    CPU example, 4 sources x 10 receivers, a new velocity every evaluation: eik_gradient
+    (upload + call) against a captured plan replayed with the new velocity (eik_plan_run).
+    Host clock per evaluation, results checked identical."""
+    from eikonalsolvers import Context, Grid2DCart
+    g = Grid2DCart(hgrid=0.5, cooinit=(0.0, 0.0), grsize=(300, 220))
+    j = np.arange(1, 221)[None, :]
+    base = np.ascontiguousarray(np.broadcast_to(2.5 + 0.034 * j, g.grsize), dtype=np.float64)
+    cs = np.column_stack([0.5 * np.linspace(10, 290, 4), np.full(4, 100.0)])
+    rec = [np.column_stack([0.5 * np.linspace(8, 294, 10), np.full(10, 10.0)])] * 4
+    rng = np.random.default_rng(3)
+    vels = [base * (1.0 + 0.01 * rng.standard_normal(g.grsize)) for _ in range(args.hmc_evals + 2)]
+    ctx = Context(device)
+    try:
+        mid = ctx.upload(base, g)
+        pobs = ctx.traveltime(mid, g, cs, rec)
+        sobs = [0.01 * np.ones(p.shape) for p in pobs]
+        # plain calls: upload the new model, one eik_gradient, release
+        t_plain, ref = [], []
+        for v in vels:
+            t0 = time.perf_counter()
+            m = ctx.upload(v, g)
+            ref.append(ctx.gradient(m, g, cs, rec, pobs, sobs, "gradvel"))
+            ctx.release(m)
+            t_plain.append(time.perf_counter() - t0)
+        plan = ctx.plan_gradient(mid, g, cs, rec, "gradvel")
+        t_plan, same = [], True
+        try:
+            for v, want in zip(vels, ref):
+                t0 = time.perf_counter()
+                got = plan.run(pobs, sobs, vel=v)
+                t_plan.append(time.perf_counter() - t0)
+                same = same and np.array_equal(got[0], want[0]) and got[1] == want[1]
+        finally:
+            plan.close()
+        ctx.release(mid)
+    finally:
+        ctx.close()
+    med = lambda x: float(np.median(x[2:])) * 1e3  # noqa: E731  (first two evaluations are warm-up)
+    return {"workload": "2D Cartesian 300x220, 4 sources x 10 receivers, :gradvel, new velocity per evaluation",
+            "evaluations": args.hmc_evals, "eik_gradient_ms": med(t_plain), "plan_run_ms": med(t_plan),
+            "plan_speedup": med(t_plain) / med(t_plan), "identical_results": bool(same),
+            "timing": "host clock per evaluation (median), velocity upload included"}
 
 
 def run_serve_leg(args, device):
