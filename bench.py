@@ -270,7 +270,7 @@ def main_b200(args):
     tuned = default_tuner().apply_known(ctx, w.grd, nsrc, ep)
     launch_params = ({"round_gate": tuned["round_gate"], "ctas_per_sm": tuned["ctas_per_sm"],
                       "source": "autotuner table shipped with the package"} if tuned else
-                     {"round_gate": 2.0, "ctas_per_sm": 0, "source": "library defaults"})
+                     {"round_gate": "by size", "ctas_per_sm": 0, "source": "library defaults"})
     N = int(np.prod(w.grd.grsize))
     nd = w.grd.ndim
     cs, off, rec, po, so = flat_inputs(w, s0, s1)
@@ -360,7 +360,7 @@ def main_b200(args):
     if args.plain_sources > 0:
         npl = min(args.plain_sources, nsrc)
         if not default_tuner().apply_known(ctx, w.grd, 1, ep):
-            ctx.set_param("round_gate", 2.0)
+            ctx.set_param("round_gate", 0.0)  # the library's choice by size
             ctx.set_param("ctas_per_sm", 0)
         stp = _lib.eik_stats()
         offs = [np.array([0, off[i + 1] - off[i]], dtype=np.int64) for i in range(npl)]

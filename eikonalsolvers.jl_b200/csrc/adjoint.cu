@@ -1037,7 +1037,7 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   ra.dpsi = dpsi;
   adj_recv_kernel<<<(int)((nsrc + 63) / 64), 64, 0, st>>>(ra);
   if (!ctx->capturing) cudaEventRecord(ctx->evk[4], st);
-  CUDA_OK(ctx, nd == 3 ? launch_adj_solve<3>(aa, ctx->solve_sms(), st) : launch_adj_solve<2>(aa, ctx->solve_sms(), st));
+  CUDA_OK(ctx, nd == 3 ? launch_adj_solve<3>(aa, fw.sms, st) : launch_adj_solve<2>(aa, fw.sms, st));
   if (!ctx->capturing) cudaEventRecord(ctx->evk[5], st);
   adj_check_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, N, fw.fb.err);
   CUDA_OK(ctx, cudaGetLastError());

@@ -363,7 +363,10 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   const void* hp_src = stage_host(ctx, hp.data(), sizeof(CoarseProblem) * nsrc);
   if (!hp_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
   CUDA_OK(ctx, cudaMemcpyAsync(dp, hp_src, sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
-  problem_scale_kernel<<<(int)((nsrc + 127) / 128), 128, 0, st>>>(dp, (int)nsrc, m.dstat + 2, ctx->round_gate, hmin,
+  const unsigned long long work = (unsigned long long)nsrc * (unsigned long long)N;
+  const double gate = ctx->gate_for(work);
+  const int sms = ctx->sms_for(work);
+  problem_scale_kernel<<<(int)((nsrc + 127) / 128), 128, 0, st>>>(dp, (int)nsrc, m.dstat + 2, gate, hmin,
                                                                   g.nd);
   CUDA_OK(ctx, cudaMemsetAsync(fb.err, 0, sizeof(uint32_t) * 4, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.out, 0, sizeof(SrcOut) * nsrc, st));
@@ -373,7 +376,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     launch_fine(fb, st);
   } else if (refine) {
     // the windows as round-solver problems, then the heap's stop reconstructed from keys
-    launch_fine_setup(fb, fprobs, m.dstat + 2, ctx->round_gate, fseed_lin, fseed_tt, fslow, fkL, fkd, st);
+    launch_fine_setup(fb, fprobs, m.dstat + 2, gate, fseed_lin, fseed_tt, fslow, fkL, fkd, st);
     SolveArgs fsa = sa;
     fsa.probs = fprobs;
     fsa.rs.stride = (unsigned long long)fb.nfmax;
@@ -381,7 +384,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     fsa.node_evals = sa.activations + 7;
     launch_rounds_init(fsa, st);
     launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
-    CUDA_OK(ctx, launch_coarse_solve(fsa, ctx->solve_sms(), ctx->ctas_per_sm, ctx->fwd_queue, st));
+    CUDA_OK(ctx, launch_coarse_solve(fsa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
     launch_fine_select(fb, fprobs, ftie, st);
     // stops decided by exact ties: the heap is replayed for the flagged sources only, the
     // flags staying on the device (no host round trip between the stages)
@@ -396,7 +399,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
   CUDA_OK(ctx, cudaGetLastError());
   if (!ctx->capturing) cudaEventRecord(ctx->evk[2], st);
-  CUDA_OK(ctx, launch_coarse_solve(sa, ctx->solve_sms(), ctx->ctas_per_sm, ctx->fwd_queue, st));
+  CUDA_OK(ctx, launch_coarse_solve(sa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
   if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
   fw->fb = fb;
@@ -409,6 +412,8 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   fw->nsrc = nsrc;
   fw->fine_tie = (refine && !ctx->fine_replay) ? ftie : nullptr;
   fw->launches = nlaunch;
+  fw->gate = gate;
+  fw->sms = sms;
   if (stats) stats->launches += nlaunch;
   return EIK_OK;
 }
@@ -518,7 +523,7 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
   if (!ctx || !name) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (std::strcmp(name, "round_gate") == 0) {
-    if (!(value > 0.0 && value < 1e6)) return fail(ctx, EIK_ERR_ASSERT, "round_gate must be in (0, 1e6)");
+    if (!(value >= 0.0 && value < 1e6)) return fail(ctx, EIK_ERR_ASSERT, "round_gate must be in [0, 1e6)");
     ctx->round_gate = value;
     return EIK_OK;
   }
@@ -544,7 +549,7 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
     return EIK_OK;
   }
   if (std::strcmp(name, "sm_fraction") == 0) {
-    if (!(value > 0.0 && value <= 1.0)) return fail(ctx, EIK_ERR_ASSERT, "sm_fraction must be in (0, 1]");
+    if (!(value >= 0.0 && value <= 1.0)) return fail(ctx, EIK_ERR_ASSERT, "sm_fraction must be in [0, 1]");
     ctx->sm_fraction = value;
     return EIK_OK;
   }

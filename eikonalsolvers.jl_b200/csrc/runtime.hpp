@@ -55,6 +55,8 @@ struct ForwardState {
   long long nsrc = 0;
   const uint8_t* fine_tie = nullptr;  // per-source replay flags of the refined start-up (device)
   int launches = 0;                   // kernels the forward stage launched
+  double gate = 2.0;                  // round width used (units of smallest spacing x slowness)
+  int sms = 1;                        // SMs of the persistent solves of this call
   std::vector<SrcOut> host_out;
 };
 
@@ -100,14 +102,22 @@ struct eik_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // whole call
   cudaEvent_t evk[6] = {};                    // start-up stage, coarse solve, adjoint solve
-  double round_gate = 2.0;  // forward round width in units of (smallest spacing x smallest slowness)
+  double round_gate = 0.0;  // forward round width in units of (smallest spacing x smallest slowness); 0 = by size
   int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
   int fwd_queue = -1;        // per-warp evaluation queue of the forward solve: -1 by size, 0 off, 1 on
-  double sm_fraction = 1.0; // share of the SMs the persistent (cooperative) solves of this context use
+  double sm_fraction = 0.0; // share of the SMs the persistent (cooperative) solves use; 0 = by size
   double ray_room = 3.0;     // room of a ray in its first tracing pass, in straight-line lengths
   bool fine_replay = false; // refined start-up by exact heap replay for every source (else only on ties)
-  int solve_sms() const {
-    const int n = (int)(sm_fraction * (double)nsm + 0.5);
+  // Launch parameters of a call whose coarse solve has `work` node-sources: the values set
+  // on the context, else chosen by size. Small calls are bound by their rounds (each closed
+  // by a grid barrier over all resident CTAs), so they take wider rounds on fewer SMs.
+  static constexpr unsigned long long SMALL_WORK = 1ull << 22;
+  double gate_for(unsigned long long work) const {
+    return round_gate > 0.0 ? round_gate : (work < SMALL_WORK ? 8.0 : 2.0);
+  }
+  int sms_for(unsigned long long work) const {
+    const double f = sm_fraction > 0.0 ? sm_fraction : (work < SMALL_WORK ? 0.25 : 1.0);
+    const int n = (int)(f * (double)nsm + 0.5);
     return n < 1 ? 1 : (n > nsm ? nsm : n);
   }
   std::mutex mu;

@@ -16,7 +16,7 @@ This loop serves such callers from many threads or processes on one GPU:
 * latency (submission to completion) is recorded per request; `stats()` gives p50/p99 and
   source-solves/s;
 * each call runs with the launch parameters the autotuner's table holds for its workload
-  class (the library defaults otherwise).
+  class (the library's choice by size otherwise).
 
 Results do not depend on the mix: the forward traveltimes are the unique fixed point of
 the order rule whatever the batch, and gradient requests are never merged (their
@@ -158,7 +158,7 @@ class Server:
                 mid = self._model_id(slot, batch[0].model)
                 nsrc = sum(r.nsrc for r in batch)
                 if not self.tuner.apply_known(ctx, grd, nsrc, batch[0].extraparams):
-                    ctx.set_param("round_gate", 2.0)
+                    ctx.set_param("round_gate", 0.0)  # the library's choice by size
                     ctx.set_param("ctas_per_sm", 0)
                 if batch[0].kind == "traveltime":
                     cs = np.vstack([np.atleast_2d(r.coordsrc) for r in batch])

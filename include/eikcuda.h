@@ -121,10 +121,11 @@ const char* eik_last_error(eik_ctx* ctx);
 void* eik_ctx_stream(eik_ctx* ctx);
 /* Scheduling parameters of a context (results do not depend on them, only the amount of
  * work does): "round_gate" = width of a forward round in units of (smallest node spacing x
- * smallest slowness), default 2; "sm_fraction" = share of the SMs that the persistent
- * solve kernels of this context occupy, in (0, 1], default 1 (contexts whose calls overlap
- * on one GPU, as in a serving loop, each take a share so that their solves can be resident
- * together); "ctas_per_sm" = resident CTAs per SM of the forward solve, an integer, 0 (the
+ * smallest slowness); "sm_fraction" = share of the SMs that the persistent solve kernels of
+ * this context occupy, in (0, 1] (contexts whose calls overlap on one GPU, as in a serving
+ * loop, each take a share so that their solves can be resident together). For both, 0 (the
+ * default) = chosen per call by its size: calls of fewer than 2^22 node-sources (nsrc x grid
+ * nodes) take round_gate 8 on a quarter of the SMs, larger ones round_gate 2 on all of them; "ctas_per_sm" = resident CTAs per SM of the forward solve, an integer, 0 (the
  * default) = as many as fit; "fwd_queue" = how the forward solve's warps work through their
  * entries: 1 = evaluations queued per warp and run 32 at a time, 0 = each in place, -1 (the
  * default) = the queue from 2^27 node-sources per launch up; "ray_room" = room of a ray in
