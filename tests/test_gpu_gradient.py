@@ -201,3 +201,18 @@ def test_smoothgradkern(ctx, kind, l):
     assert np.array_equal(g, O.smoothgradient(l, w.grd, g0))
     o = O.eikgradient(w.vel, w.grd, w.coordsrc, w.coordrec, w.pickobs, w.stdobs, "gradvel", extraparams=ep)
     _check((g, m), o, "gradvel")
+
+
+@pytest.mark.parametrize("maker", [_sphere2d, _sphere3d], ids=["sphere2D", "sphere3D"])
+def test_spherical_smoothgradkern(ctx, maker):
+    """Gaussian smoothing of the summed gradient on spherical grids (index-space smoothing,
+    as the reference's smoothgradient): bit-identical to the oracle's smoothing of the GPU's
+    unsmoothed gradient and within the gradient tolerance of the oracle's eikgradient."""
+    grd, vel, cs, rec = maker()
+    pobs, sobs = _obs(vel * 1.03, grd, cs, rec, ExtraParams(), sigma=0.01)
+    ep = ExtraParams(smoothgradkern=3)
+    g, m = _gpu_grad(ctx, vel, grd, cs, rec, pobs, sobs, "gradvel", ep)
+    g0, _ = _gpu_grad(ctx, vel, grd, cs, rec, pobs, sobs, "gradvel", ExtraParams())
+    assert np.array_equal(g, O.smoothgradient(3, grd, g0))
+    o = O.eikgradient(vel, grd, cs, rec, pobs, sobs, "gradvel", extraparams=ep)
+    _check((g, m), o, "gradvel")

@@ -107,3 +107,27 @@ def test_plan_pins_model_and_context_and_checks_velocity():
         plan.close()
     ctx.release(mid)
     ctx.close()
+
+
+def test_plan_on_a_spherical_grid():
+    """A plan on a Grid3DSphere model: replays with new velocities equal eik_gradient."""
+    from eikonalsolvers import Grid3DSphere
+    grd = Grid3DSphere(Δr=2.0, Δθ=0.25, Δφ=0.3, cooinit=(5800.0, 40.0, 10.0), grsize=(18, 20, 22))
+    r = np.array(grd.r)[:, None, None]
+    vel = np.ascontiguousarray(np.broadcast_to(5.0 + 0.01 * (6000.0 - r), grd.grsize))
+    cs = np.array([[5800.0 + 8.3 * 2.0, 40.0 + 9.4 * 0.25, 10.0 + 10.6 * 0.3]])
+    th, ph = np.linspace(40.3, 44.5, 3), np.linspace(10.4, 16.0, 3)
+    rec = [np.array([[5800.0 + 17 * 2.0, a, b] for a in th for b in ph])]
+    ep = ExtraParams()
+    po, so = _obs(vel * 1.02, grd, cs, rec, ep, 5)
+    vel2 = vel * (1.0 + 0.01 * np.random.default_rng(8).uniform(-1.0, 1.0, vel.shape))
+    ctx = Context(0)
+    mid = ctx.upload(vel, grd)
+    plan = ctx.plan_gradient(mid, grd, cs, rec, "gradvel", extraparams=ep)
+    try:
+        for v, vref in ((None, vel), (vel2, vel2), (vel, vel)):
+            assert _same(plan.run(po, so, vel=v), _reference(vref, grd, cs, rec, po, so, "gradvel", ep)[0])
+    finally:
+        plan.close()
+        ctx.release(mid)
+        ctx.close()

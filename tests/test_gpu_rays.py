@@ -98,3 +98,22 @@ def test_rays_that_outgrow_their_room_are_traced_again(ctx):
         ctx.set_param("ray_room", 3.0)
     for a, b in zip(got, want):
         assert all(np.array_equal(x, y) for x, y in zip(a, b))
+
+
+def test_polar_traveltime_rays(ctx):
+    """Picks and rays in one device pipeline on a Grid2DSphere model equal eik_traveltime's
+    picks and the rays of its returned grids."""
+    g = Grid2DSphere(Δr=2.0, Δθ=0.02, cooinit=(5800.0, 10.0), grsize=(40, 60))
+    r = np.array(g.r)[:, None]
+    vel = np.ascontiguousarray(np.broadcast_to(5.0 + 0.01 * (6000.0 - r), g.grsize))
+    cs = np.array([[5800.0 + 17.3 * 2.0, 10.0 + 31.4 * 0.02]])
+    rec = [np.column_stack([np.full(4, 5878.0), np.linspace(10.1, 11.1, 4)])]
+    mid = ctx.upload(vel, g)
+    try:
+        picks, rays = ctx.traveltime_rays(mid, g, cs, rec, steplen=0.5)
+        p2, tt = ctx.traveltime(mid, g, cs, rec, returntt=True)
+    finally:
+        ctx.release(mid)
+    assert all(np.array_equal(a, b) for a, b in zip(picks, p2))
+    r2 = tracerays(g, tt, cs, rec, steplen=0.5, ctx=ctx)
+    assert all(np.array_equal(x, y) for x, y in zip(rays[0], r2[0]))
