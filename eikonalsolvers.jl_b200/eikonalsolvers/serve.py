@@ -12,7 +12,12 @@ This loop serves such callers from many threads or processes on one GPU:
 * a slot that becomes free takes the oldest waiting request, together with every other
   waiting traveltime request on the same model and parameters (up to a source cap): they
   run as one batched call and the picks are split back per request;
-* a request that does not fit a slot's HBM budget fails alone (EIK_ERR_OUT_OF_BUDGET);
+* admission by device memory: with a server-wide ``hbm_budget`` every batch's device
+  footprint is estimated (``request_bytes``: the per-node-source state of the forward solve,
+  and of the adjoint for gradients, times grid nodes and sources, plus the refined windows),
+  and a slot that took a batch waits until the batch fits beside the batches in flight; a
+  batch that could not fit even alone fails with an error and the server goes on;
+* a request that does not fit a slot's own HBM budget fails alone (EIK_ERR_OUT_OF_BUDGET);
 * latency (submission to completion) is recorded per request; `stats()` gives p50/p99 and
   source-solves/s;
 * each call runs with the launch parameters the autotuner's table holds for its workload
@@ -60,6 +65,21 @@ class Request:
         return int(np.atleast_2d(self.coordsrc).shape[0])
 
 
+def request_bytes(grd, nsrc: int, kind: str, extraparams: Optional[ExtraParams] = None) -> int:
+    """Estimated device memory of one batched call: per node and source the forward's fields
+    (traveltime, codes, keys: 18 B) and round-solver state (stamp, cached front, dirty flag,
+    two worklist entries: 29 B), for gradients also the adjoint's (λ, right-hand side and
+    2·(D t) per axis: 16 + 8·ndim B); plus the refined windows ((2r+1)·ds+1 nodes per axis)."""
+    ep = extraparams or ExtraParams()
+    n = int(np.prod(grd.grsize))
+    per = 47 + ((16 + 8 * grd.ndim) if kind == "gradient" else 0)
+    fine = 0
+    if ep.refinearoundsrc:
+        side = (2 * ep.grdrefpars.noderadius + 1) * ep.grdrefpars.downscalefactor + 1
+        fine = side ** grd.ndim * 48
+    return int(nsrc) * (n * per + fine)
+
+
 def _ep_key(ep: Optional[ExtraParams]):
     if ep is None:
         return None
@@ -71,8 +91,12 @@ class Server:
     """Serves `Request`s on one GPU with `slots` concurrent worker contexts."""
 
     def __init__(self, device: int = 0, slots: int = 2, hbm_budget_per_slot: int = 0,
-                 max_batch_sources: int = 64, context_factory=None, tuner=None):
+                 max_batch_sources: int = 64, context_factory=None, tuner=None, hbm_budget: int = 0):
         self.slots = max(1, int(slots))
+        self.hbm_budget = int(hbm_budget)  # device bytes the batches in flight may take together (0 = no limit)
+        self._inflight = 0
+        self.max_inflight_seen = 0
+        self._mem_cv = threading.Condition()  # admission waits here, apart from the request queue
         # launch parameters per workload class (autotuner table; results do not depend on them)
         self.tuner = tuner if tuner is not None else default_tuner()
         self.max_batch_sources = int(max_batch_sources)
@@ -144,12 +168,45 @@ class Server:
                 self._queue = keep
             return batch
 
+    def _admit(self, need: int) -> bool:
+        """Waits until `need` bytes fit beside the batches in flight; False if they never can."""
+        if self.hbm_budget <= 0:
+            return True
+        if need > self.hbm_budget:
+            return False
+        with self._mem_cv:
+            while self._inflight + need > self.hbm_budget:
+                self._mem_cv.wait()
+            self._inflight += need
+            self.max_inflight_seen = max(self.max_inflight_seen, self._inflight)
+        return True
+
+    def _release(self, need: int):
+        if self.hbm_budget <= 0:
+            return
+        with self._mem_cv:
+            self._inflight -= need
+            self._mem_cv.notify_all()
+
     def _worker(self, slot: int):
         ctx = self._ctx[slot]
         while True:
             batch = self._take()
             if batch is None:
                 return
+            grd0 = self._models[batch[0].model][1]
+            need = request_bytes(grd0, sum(r.nsrc for r in batch), batch[0].kind, batch[0].extraparams)
+            if not self._admit(need):
+                err = MemoryError(f"request needs ~{need} bytes of device memory, the server's budget is "
+                                  f"{self.hbm_budget}")
+                t1 = time.perf_counter()
+                with self._cv:
+                    for r in batch:
+                        r.t_start = r.t_done = t1
+                        self._done.append(r)
+                for r in batch:
+                    r.future.set_exception(err)
+                continue
             t0 = time.perf_counter()
             for r in batch:
                 r.t_start = t0
@@ -176,6 +233,7 @@ class Server:
                 err = None
             except Exception as e:  # the request fails, the server goes on
                 err = e
+            self._release(need)
             t1 = time.perf_counter()
             with self._cv:
                 self._busy_s += t1 - t0

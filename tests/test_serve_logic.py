@@ -102,3 +102,34 @@ def test_slots_get_an_sm_share_and_unknown_models_are_refused(grd):
     with pytest.raises(KeyError):
         srv.submit(_req("traveltime", [1.0], model="zzz"))
     srv.close()
+
+
+def test_admission_by_device_memory(grd):
+    """With a server-wide HBM budget that holds one gradient batch but not two, gradients run
+    one at a time while the slots still take them; a request larger than the whole budget fails
+    alone; everything else completes."""
+    from eikonalsolvers.serve import request_bytes
+    one = request_bytes(grd, 1, "gradient")
+    srv = Server(slots=3, context_factory=FakeContext, hbm_budget=int(1.5 * one))
+    try:
+        srv.register_model("a", np.ones(grd.grsize), grd)
+        futs = [srv.submit(_req("gradient", [1.0 + i])) for i in range(6)]
+        big = srv.submit(_req("gradient", [1.0, 2.0]))  # two sources: about twice the budget / 1.5
+        for f in futs:
+            g, m = f.result(timeout=10)
+            assert g.shape == grd.grsize
+        with pytest.raises(MemoryError):
+            big.result(timeout=10)
+        assert 0 < srv.max_inflight_seen <= srv.hbm_budget
+        assert srv.max_inflight_seen < 2 * one  # never two gradients in flight at once
+    finally:
+        srv.close()
+
+
+def test_request_bytes_scales_with_work(grd):
+    from eikonalsolvers import ExtraParams
+    from eikonalsolvers.serve import request_bytes
+    t1 = request_bytes(grd, 1, "traveltime")
+    assert request_bytes(grd, 4, "traveltime") == 4 * t1
+    assert request_bytes(grd, 1, "gradient") > t1
+    assert request_bytes(grd, 1, "traveltime", ExtraParams(refinearoundsrc=False)) < t1
