@@ -592,8 +592,13 @@ def main_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": "oracle (C++ restatement of the reference FMM + CSR adjoint), "
-                                   "threaded by source groups as :sharedmem"},
+            "config": {"workload": f"3D Cartesian eikgradient :gradvelandsrcloc, {w.grd.grsize[0]}^3, "
+                                   f"hgrid {w.grd.hgrid}, 4-layer model, {args.nsrc} sources per GPU, 400 receivers, "
+                                   "default ExtraParams (refined start-up ds=5 r=3, smoothing radius 3)",
+                       "sources_per_gpu": args.nsrc, "nodes": int(np.prod(w.grd.grsize)),
+                       "implementation": "oracle (C++ restatement of the reference FMM + CSR adjoint), "
+                                         "threaded by source groups as :sharedmem; each step a bounded sample "
+                                         "of the workload (see cpu_baseline.sample)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
