@@ -13,6 +13,8 @@
 // different host threads) race on it and give wrong results: serialise them.
 // The first call on each device does a one-time set-up (it looks up the array's device
 // address with cudaGetSymbolAddress); make that first call before any stream capture.
+// Every call copies the receiver offsets from host memory, reads its error word back to the
+// host and synchronises its stream: it blocks the calling thread until the misfit is written.
 #include <mutex>
 
 #include "../../include/eikcuda.h"

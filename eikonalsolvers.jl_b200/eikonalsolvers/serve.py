@@ -156,11 +156,16 @@ class Server:
             if head.kind == "traveltime":
                 n = head.nsrc
                 key = (head.model, _ep_key(head.extraparams))
+                grd = self._models[head.model][1]
                 keep = deque()
                 while self._queue:
                     r = self._queue.popleft()
+                    # with a device-memory budget, a merged batch must still fit it: requests
+                    # that fit alone are not refused only because they were batched together
+                    fits = (self.hbm_budget <= 0 or
+                            request_bytes(grd, n + r.nsrc, "traveltime", head.extraparams) <= self.hbm_budget)
                     if (r.kind == "traveltime" and (r.model, _ep_key(r.extraparams)) == key
-                            and n + r.nsrc <= self.max_batch_sources):
+                            and n + r.nsrc <= self.max_batch_sources and fits):
                         batch.append(r)
                         n += r.nsrc
                     else:

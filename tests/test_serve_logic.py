@@ -133,3 +133,25 @@ def test_request_bytes_scales_with_work(grd):
     assert request_bytes(grd, 4, "traveltime") == 4 * t1
     assert request_bytes(grd, 1, "gradient") > t1
     assert request_bytes(grd, 1, "traveltime", ExtraParams(refinearoundsrc=False)) < t1
+
+
+def test_traveltime_batches_are_capped_by_the_memory_budget(grd):
+    """Several 1-source traveltime requests on one model whose sum exceeds the server's budget
+    while each fits alone: they are merged only as far as the budget allows, so none fails."""
+    from eikonalsolvers.serve import request_bytes
+    FakeContext.calls = []
+    one = request_bytes(grd, 1, "traveltime")
+    srv = Server(slots=1, max_batch_sources=64, context_factory=FakeContext, hbm_budget=int(2.5 * one))
+    try:
+        srv.register_model("a", np.ones(grd.grsize), grd)
+        assert request_bytes(grd, 1, "gradient") <= srv.hbm_budget
+        blocker = srv.submit(_req("gradient", [9.0]))  # keeps the only slot busy meanwhile
+        futs = [srv.submit(_req("traveltime", [1.0 + i])) for i in range(5)]
+        blocker.result(timeout=10)
+        res = [f.result(timeout=10) for f in futs]
+        assert [float(p[0][0]) for p in res] == [1.0 + i for i in range(5)]
+        sizes = [n for (k, n) in FakeContext.calls if k == "traveltime"]
+        assert sum(sizes) == 5 and max(sizes) <= 2
+        assert srv.max_inflight_seen <= srv.hbm_budget
+    finally:
+        srv.close()

@@ -18,7 +18,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from eikonalsolvers import Context, Grid3DCart, _lib
+from eikonalsolvers import Context, Grid2DSphere, Grid3DCart, Grid3DSphere, _lib
 from eikonalsolvers import configs as CF
 
 pytestmark = pytest.mark.gpu
@@ -39,6 +39,28 @@ def _case(kind):
     if kind == "2D":
         w = CF.cfg2(scale=0.125, nsrc=5)
         return w.grd, w.vel, w.coordsrc, w.coordrec
+    if kind == "sphere2D":
+        # polar grid; receivers include the last node of both axes (the i == n corner rule)
+        grd = Grid2DSphere(Δr=2.0, Δθ=0.25, cooinit=(5800.0, 10.0), grsize=(40, 50))
+        r = np.array(grd.r)[:, None]
+        vel = np.ascontiguousarray(np.broadcast_to(5.0 + 0.01 * (6000.0 - r), grd.grsize))
+        cs = np.array([[5800.0 + 17.3 * 2.0, 10.0 + 21.4 * 0.25], [5800.0 + 9.0 * 2.0, 10.0 + 30.6 * 0.25],
+                       [5800.0 + 25.5 * 2.0, 10.0 + 7.2 * 0.25]])
+        th = np.linspace(10.5, grd.θ[-1], 9)
+        rec = np.column_stack([np.full(9, grd.r[-1]), th])
+        rec = np.vstack([rec, [[5830.3, grd.θ[-1]], [grd.r[-1], grd.θ[-1]]]])
+        return grd, vel, cs, [rec.copy() for _ in range(3)]
+    if kind == "sphere3D":
+        grd = Grid3DSphere(Δr=2.0, Δθ=0.25, Δφ=0.3, cooinit=(5800.0, 40.0, 10.0), grsize=(18, 20, 22))
+        r = np.array(grd.r)[:, None, None]
+        vel = np.ascontiguousarray(np.broadcast_to(5.0 + 0.01 * (6000.0 - r), grd.grsize))
+        cs = np.array([[5800.0 + 8.3 * 2.0, 40.0 + 9.4 * 0.25, 10.0 + 10.6 * 0.3],
+                       [5800.0 + 4.6 * 2.0, 40.0 + 12.2 * 0.25, 10.0 + 6.3 * 0.3],
+                       [5800.0 + 12.1 * 2.0, 40.0 + 5.7 * 0.25, 10.0 + 15.2 * 0.3]])
+        th = np.linspace(40.3, grd.θ[-1], 4)
+        ph = np.linspace(10.4, grd.φ[-1], 4)
+        rec = np.array([[grd.r[-1], a, b] for a in th for b in ph] + [[5810.7, grd.θ[-1], grd.φ[-1]]])
+        return grd, vel, cs, [rec.copy() for _ in range(3)]
     grd = Grid3DCart(hgrid=0.1, cooinit=(0.0, 0.0, 0.0), grsize=(24, 20, 18))
     vel = CF.layered_3d(grd.grsize, seed=5)
     rng = np.random.default_rng(21)
@@ -71,7 +93,7 @@ def _noalloc(L, torch, grd, tt, recs, pobs, sobs):
     return rc, float(out.item())
 
 
-@pytest.mark.parametrize("kind", ["2D", "3D"])
+@pytest.mark.parametrize("kind", ["2D", "3D", "sphere2D", "sphere3D"])
 def test_noalloc_misfit_matches_regular_entry_points(kind):
     torch = pytest.importorskip("torch")
     grd, vel, cs, recs = _case(kind)
@@ -88,11 +110,11 @@ def test_noalloc_misfit_matches_regular_entry_points(kind):
         rc, m1 = _noalloc(L, torch, grd, tt, recs, pobs, sobs)
         assert rc == 0, _lib.load().eik_last_error(None)
         ref1 = _host_misfit(picks, pobs, sobs)
-        _, mg = ctx.gradient(mid, grd, cs, recs, pobs, sobs, "gradvel")
+        _, mg = ctx.gradient(mid, grd, cs, recs, pobs, sobs, "gradvel")  # gradvel runs on every grid kind
         assert abs(m1 - ref1) <= MISFIT_RTOL * abs(ref1), (m1, ref1)
         assert abs(m1 - mg) <= MISFIT_RTOL * abs(mg), (m1, mg)
         # call 2, right after: fewer sources and other observations
-        k = len(tt) - 2
+        k = max(1, len(tt) - 2)
         pobs2 = [o + 0.02 for o in pobs[:k]]
         sobs2 = [2.0 * s for s in sobs[:k]]
         rc, m2 = _noalloc(L, torch, grd, tt[:k], recs[:k], pobs2, sobs2)
