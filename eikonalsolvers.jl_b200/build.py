@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -34,17 +35,21 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
+    objs = [os.path.join(LIBDIR, src.replace(".cu", ".o")) for src in SOURCES]
+
+    def compile_one(src, obj):
         cmd = [NVCC, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
+        return src, subprocess.run(cmd, capture_output=True, text=True)
+
+    # the translation units compile independently: one nvcc process each
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda so: compile_one(*so), zip(SOURCES, objs)))
+    for src, r in results:
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed on {src}")
         if verbose:
             sys.stderr.write(r.stderr)
-        objs.append(obj)
     cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "--cudart=static", "-shared",
            "-o", LIB, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)

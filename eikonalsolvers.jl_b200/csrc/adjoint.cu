@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) adj_rounds_kernel(AdjArgs aa) {
       const unsigned int idx = base + lane;
       unsigned int rel[6] = {~0u, ~0u, ~0u, ~0u, ~0u, ~0u};
       if (idx < n) {
-        const unsigned int gid = (unsigned int)(L[idx] >> 32);
+        const unsigned int gid = (unsigned int)(__ldcg(L + idx) >> 32);
         const int prob = (int)(gid / N);
         const unsigned long long gb = (unsigned long long)prob * N;
         adj_node<ND>(aa, prob, (long long)(gid - gb), gb, rel);
@@ -1019,7 +1019,7 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   AdjArgs aa;
   aa.sa = fw.sa;
   aa.ap = dap;
-  aa.sa.rs.max_rounds = 1 << 26;
+  aa.sa.rs.max_rounds = ctx->max_rounds > 0 ? ctx->max_rounds : (1 << 26);
   aa.sa.rs.rounds = fw.sa.rs.rounds + 1;  // the forward's count stays readable
   adj_rounds_init_kernel<<<1, 1, 0, st>>>(aa.sa);
   adj_prep_kernel<<<2 * ctx->nsm * 8, 256, 0, st>>>(dprobs, dap, (int)nsrc, N, aa.sa);

@@ -14,6 +14,7 @@
 
 #include "../../include/eikcuda.h"
 #include "kernels.cuh"
+#include "rounds.cuh"
 #include "runtime.hpp"
 
 namespace eik {
@@ -339,7 +340,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     sa.rs.rounds = (int32_t*)(rc32 + 8);
     sa.rs.visits = reinterpret_cast<unsigned long long*>(rc32 + 12);  // 8-byte aligned: 7 counters
   }
-  sa.rs.max_rounds = 1 << 24;
+  sa.rs.max_rounds = ctx->max_rounds > 0 ? ctx->max_rounds : (1 << 24);
   sa.rs.stride = (unsigned long long)N;
   sa.err = fb.err;
   sa.probs = dp;
@@ -548,12 +549,52 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
     ctx->fwd_queue = (int)value;
     return EIK_OK;
   }
+  if (std::strcmp(name, "max_rounds") == 0) {
+    if (!(value >= 0.0 && value <= (double)(1 << 30) && value == (double)(long long)value))
+      return fail(ctx, EIK_ERR_ASSERT, "max_rounds must be an integer in [0, 2^30] (0 = the library's limit)");
+    ctx->max_rounds = (int)value;
+    return EIK_OK;
+  }
   if (std::strcmp(name, "sm_fraction") == 0) {
     if (!(value >= 0.0 && value <= 1.0)) return fail(ctx, EIK_ERR_ASSERT, "sm_fraction must be in [0, 1]");
     ctx->sm_fraction = value;
     return EIK_OK;
   }
   return fail(ctx, EIK_ERR_ASSERT, "unknown parameter '%s'", name);
+}
+
+}  // extern "C"
+
+namespace eik {
+// A bounded wait on a flag that nothing sets: the wait limit of the persistent solves
+// (global timer, then an error bit instead of a trap), exercised on its own.
+__global__ void selftest_wait_kernel(const unsigned int* flag, long long timeout_ns, uint32_t* err) {
+  const long long t0 = gtimer_ns();
+  while (*(volatile const unsigned int*)flag == 0u) {
+    if (gtimer_ns() - t0 > timeout_ns) {
+      atomicOr(err, ERRB_QUEUE_TIMEOUT);
+      return;
+    }
+    __nanosleep(1000);
+  }
+}
+}  // namespace eik
+
+extern "C" {
+
+int eik_selftest_wait(eik_ctx* ctx, double timeout_s) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  if (!(timeout_s >= 1e-3 && timeout_s <= 10.0)) return fail(ctx, EIK_ERR_ASSERT, "timeout_s must be in [0.001, 10]");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  int rc = EIK_OK;
+  unsigned int* flag = (unsigned int*)ctx->scratch.get("selftest_flag", 2 * sizeof(unsigned int), &rc);
+  if (!flag) return fail(ctx, rc, "scratch allocation failed");
+  uint32_t* err = flag + 1;
+  CUDA_OK(ctx, cudaMemsetAsync(flag, 0, 2 * sizeof(unsigned int), ctx->stream));
+  selftest_wait_kernel<<<1, 1, 0, ctx->stream>>>(flag, (long long)(timeout_s * 1e9), err);
+  CUDA_OK(ctx, cudaGetLastError());
+  return err_to_rc(ctx, read_err(ctx, err));
 }
 
 const char* eik_last_error(eik_ctx* ctx) {

@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
     double* thr_cur = a.rs.thr + (size_t)(r & 1) * a.nprob;
     if (blockIdx.x == 0)
       for (int p = threadIdx.x; p < a.nprob; p += blockDim.x)
-        thr_cur[p] = fmax(thr_prev[p], __longlong_as_double((long long)ld_volatile(nm + p)) + a.probs[p].delta);
+        thr_cur[p] = fmax(__ldcg(thr_prev + p), __longlong_as_double((long long)ld_volatile(nm + p)) + a.probs[p].delta);
     if constexpr (QUEUE) {
       // Visits whose front still stands (nothing they read has changed) are settled when
       // taken; the others wait in a per-warp queue in shared memory and are evaluated 32 at a
@@ -393,12 +393,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
           bool queue = false;
           unsigned long long e = 0;
           if (idx < n) {
-            e = L[idx];
+            e = __ldcg(L + idx);
             const unsigned int gid = (unsigned int)(e >> 32);
             const double ef = (double)__uint_as_float((unsigned int)e);
             prob = (int)(gid / N);
             l = (long long)(gid - (unsigned long long)prob * N);
-            const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) +
+            const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) +
                                                       a.probs[prob].delta);
             if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
               front = ef;
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
             prob = (int)(gid / N);
             l = (long long)(gid - (unsigned long long)prob * N);
             const CoarseProblem& P = a.probs[prob];
-            const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
+            const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
             const unsigned long long gb = (unsigned long long)prob * N;
             dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
                              : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
@@ -502,14 +502,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
         int prob = 0;
         long long l = 0;
         if (idx < n) {
-          const unsigned long long e = L[idx];
+          const unsigned long long e = __ldcg(L + idx);
           const unsigned int gid = (unsigned int)(e >> 32);
           const double ef = (double)__uint_as_float((unsigned int)e);
           prob = (int)(gid / N);
           l = (long long)(gid - (unsigned long long)prob * N);
           const CoarseProblem& P = a.probs[prob];
           // window of one round width above the smallest pending front, never moving back
-          const double T = fmax(thr_prev[prob], __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
+          const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
           const unsigned long long gb = (unsigned long long)prob * N;
           if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
             // still waiting and nothing it reads has changed: its front stands

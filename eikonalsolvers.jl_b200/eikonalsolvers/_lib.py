@@ -24,7 +24,26 @@ EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
             "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc",
             "eik_ctx_set_param", "eik_plan_gradient", "eik_plan_run", "eik_plan_destroy", "eik_tracerays",
-            "eik_traveltime_rays"]
+            "eik_traveltime_rays", "eik_selftest_wait"]
+
+# eik_stats.warn_mask bits and the reference's @warn messages they stand for
+WARNINGS = {
+    0x1: "negative discriminant in the local traveltime update: one-dimensional update used "
+         "(eikforward2D.jl:342, eikforward3D.jl:429)",
+    0x2: "a source lies exactly halfway between grid nodes on an axis: it was shifted by 1e-4 of the "
+         "spacing (eikmainfwd.jl:1298)",
+    0x4: "the refined grid reached a border before the coarse grid took over (eikmainfwd.jl:731)",
+    0x8: "a source coordinate is aligned with the grid: it was shifted by 1e-6 of the spacing for its "
+         "derivative (eikmaingrad.jl:1250)",
+    0x10: "a source lies on a node: the derivative of the traveltime there is set to zero "
+          "(eikmaingrad.jl:1260)",
+    0x20: "the refined grid covered the whole model: no edge stop",
+}
+
+
+def warn_mask_messages(mask: int):
+    """Messages of the reference's @warn sites whose bits are set in an eik_stats.warn_mask."""
+    return [msg for bit, msg in WARNINGS.items() if mask & bit]
 
 
 class EikError(RuntimeError):
@@ -88,6 +107,8 @@ def load():
                                           C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
         L.eik_ttimemisfit_noalloc.argtypes = [C.POINTER(eik_grid), C.c_int64, P, P, P, P, P, P, P]
         L.eik_ttimemisfit_noalloc.restype = C.c_int
+        L.eik_selftest_wait.argtypes = [P, C.c_double]
+        L.eik_selftest_wait.restype = C.c_int
         L.eik_ctx_set_param.argtypes = [P, C.c_char_p, C.c_double]
         L.eik_ctx_set_param.restype = C.c_int
         L.eik_ctx_stream.argtypes = [P]

@@ -16,12 +16,22 @@ from __future__ import annotations
 
 import ctypes as C
 import threading
+import warnings
 from typing import Optional
 
 import numpy as np
 
 from . import _lib
 from .structs import WHICHGRAD, ExtraParams, normalize_inputs
+
+
+class EikonalWarning(UserWarning):
+    """A condition the reference reports with @warn (the call still returns its result)."""
+
+
+def _warn(st) -> None:
+    for msg in _lib.warn_mask_messages(int(st.warn_mask)):
+        warnings.warn(msg, EikonalWarning, stacklevel=3)
 
 
 class Context:
@@ -38,6 +48,10 @@ class Context:
         """Scheduling parameter of this context (see eik_ctx_set_param)."""
         _lib.check(self.L.eik_ctx_set_param(self.h, name.encode(), float(value)), self.h)
 
+    def selftest_wait(self, timeout_s: float = 0.2) -> int:
+        """Runs one bounded device wait on a flag that nothing sets (eik_selftest_wait) and
+        returns its status: EIK_ERR_TIMEOUT (-6) when the wait limit works."""
+        return int(self.L.eik_selftest_wait(self.h, float(timeout_s)))
     def close(self):
         if self.h:
             self.L.eik_ctx_destroy(self.h)
@@ -120,6 +134,7 @@ class Context:
                                    C.byref(ep), _lib.ptr(picks), _lib.ptr(ttg), C.byref(st))
         self.last_stats = st
         _lib.check(rc, self.h)
+        _warn(st)
         out = [picks[recoff[s]:recoff[s + 1]].copy() for s in range(nsrc)]
         if returntt:
             return out, [ttg[s * N:(s + 1) * N].reshape(grd.grsize, order="F").copy() for s in range(nsrc)]
@@ -161,6 +176,7 @@ class Context:
                                  _lib.ptr(gs), _lib.ptr(misf), C.byref(st))
         self.last_stats = st
         _lib.check(rc, self.h)
+        _warn(st)
         gradvel = gv.reshape(grd.grsize, order="F") if gv is not None else None
         gradsrc = gs.reshape(nsrc, grd.ndim) if gs is not None else None
         if wg == "gradvel":

@@ -131,9 +131,19 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * default) = the queue from 2^27 node-sources per launch up; "ray_room" = room of a ray in
  * the single tracing pass, in multiples of its straight-line length (default 3; rays that
  * outgrow it are traced again); "fine_replay" = 1 replays the refined start-up's heap for every
- * source instead of only where an exact tie decides its stop (default 0). Returns
- * EIK_ERR_ASSERT for an unknown name or a value out of range. */
+ * source instead of only where an exact tie decides its stop (default 0); "max_rounds" = round
+ * limit of the persistent forward and adjoint solves, an integer, 0 (the default) = the
+ * library's (2^24 forward, 2^26 adjoint); a solve that reaches it stops on the device and the
+ * call returns EIK_ERR_NOT_CONVERGED, the context staying usable. Returns EIK_ERR_ASSERT for
+ * an unknown name or a value out of range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
+
+/* No counterpart in the reference: failure-detection self-test. Runs, on the context's
+ * stream, one device wait of the kind the persistent solves use (bounded by the global
+ * timer) on a flag that nothing sets, with a limit of timeout_s seconds (in [0.001, 10]),
+ * and returns what such a wait reports when it runs out: EIK_ERR_TIMEOUT, the kernel having
+ * returned and the context staying usable. */
+int eik_selftest_wait(eik_ctx* ctx, double timeout_s);
 
 /* Uploads a velocity model (host, column-major, FP64) and keeps it resident. Checks
  * all(vel.>0) (eikmainfwd.jl:45). */

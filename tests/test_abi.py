@@ -59,3 +59,19 @@ def test_extra_defaults_match_reference():
     e = _lib.extra_struct(None)
     assert (e.refinearoundsrc, e.downscalefactor, e.noderadius, e.radiussmoothgradsrc,
             e.smoothgradkern, e.parallelkind) == (1, 5, 3, 3, 0, 0)
+
+
+def test_warn_mask_messages_follow_the_reference_warn_sites():
+    import warnings
+    from eikonalsolvers import EikonalWarning, _lib
+    from eikonalsolvers.api import _warn
+    assert _lib.warn_mask_messages(0) == []
+    msgs = _lib.warn_mask_messages(0x2 | 0x10)
+    assert len(msgs) == 2 and "halfway" in msgs[0] and "node" in msgs[1]
+    st = _lib.eik_stats()
+    st.warn_mask = 0x1
+    with warnings.catch_warnings(record=True) as rec:
+        warnings.simplefilter("always")
+        _warn(st)
+    assert len(rec) == 1 and issubclass(rec[0].category, EikonalWarning)
+    assert "discriminant" in str(rec[0].message)
