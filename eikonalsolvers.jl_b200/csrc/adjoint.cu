@@ -386,6 +386,9 @@ struct SrcTermArgs {
   int refine;
   int whichgrad;
   int ngroups;          // consecutive source groups with their own gradient buffer
+  int s0;               // index, in the whole call, of this chunk's first source
+  int nsrc_total;       // sources of the whole call (groups are those of the whole call)
+  const double* prevbuf;  // N: the group buffer before this chunk (its previous source's final field), or null
   const CoarseProblem* probs;
   const AdjProblem* ap;
   const ForwardBatch* fb;
@@ -820,18 +823,25 @@ __device__ int group_start(int nsrc, int nw, int s) {
 // current source's points (eikmaingrad.jl:182, 417-479), so a source point starts from
 // the previous source's smoothed value there. The carried value is a short recurrence over
 // the run of earlier sources sharing the point; one thread per (source, point).
+//
+// A call split into chunks of sources runs this per chunk with the sources numbered within
+// the chunk: a group that began in an earlier chunk starts here from the buffer as the
+// previous chunk left it (prevbuf: its last source's final field), which is the value the
+// recurrence over the earlier sources produces.
 __global__ void adj_carry_kernel(SrcTermArgs sa, int R, double* carry) {
   const int s = blockIdx.x;
   const ForwardBatch& fb = *sa.fb;
   const GridDesc& g = sa.g;
-  const int gs = group_start(sa.nsrc, sa.ngroups, s);
+  const int gs = group_start(sa.nsrc_total, sa.ngroups, sa.s0 + s) - sa.s0;  // < 0: began in an earlier chunk
+  const int lo = gs > 0 ? gs : 0;
   for (int k = threadIdx.x; k < fb.out[s].nseeds; k += blockDim.x) {
     const long long l = fb.seed_lin[(size_t)s * fb.seedcap + k];
     const int i = (int)(l % g.n[0]), j = (int)((l / g.n[0]) % g.n[1]), kz = (int)(l / ((long long)g.n[0] * g.n[1]));
     int m = s - 1;
-    while (m >= gs && seed_index(fb, m, l) >= 0) m--;
+    while (m >= lo && seed_index(fb, m, l) >= 0) m--;
     double c = 0.0;
-    if (m >= gs) c = smooth_factor(g, sa.coordsrc + (size_t)m * g.nd, R, i, j, kz) * sa.ap[m].lam[l];
+    if (m >= lo) c = smooth_factor(g, sa.coordsrc + (size_t)m * g.nd, R, i, j, kz) * sa.ap[m].lam[l];
+    else if (gs < 0 && sa.prevbuf) c = sa.prevbuf[l];
     for (int q = m + 1; q < s; q++) {
       const int kq = seed_index(fb, q, l);
       c = smooth_factor(g, sa.coordsrc + (size_t)q * g.nd, R, i, j, kz) * (c + sa.gsrcnode[(size_t)q * fb.seedcap + kq]);
@@ -878,16 +888,29 @@ __global__ void adj_smooth_kernel(SrcTermArgs sa, int R) {
   }
 }
 
+// Running state of the ordered sums over a call's sources, carried from chunk to chunk:
+// the sum of the finished groups, the current group's partial sum, whether a group has
+// finished yet, and the first source of the current group.
+struct SumState {
+  double* acc;  // N (or 1 for the misfit), null for a call in one chunk
+  double* tot;
+  int first_group;
+  int gcur;
+  int final_chunk;
+};
+
 // Σ over sources in the reference's order: within a group in source order, then the
-// group sums in group order (eikmaingrad.jl:137-150).
-__global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int nw, long long N, double* out) {
+// group sums in group order (eikmaingrad.jl:137-150). Sources s0 .. s0+nsrc-1 of a call of
+// nsrc_total; the last chunk writes the total.
+__global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int s0, int nsrc_total, int nw, long long N,
+                               SumState ss, double* out) {
   for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < N; l += (long long)gridDim.x * blockDim.x) {
-    double tot = 0.0, acc = 0.0;
-    int gcur = 0;
-    bool first_group = true;
+    double tot = ss.tot ? ss.tot[l] : 0.0, acc = ss.acc ? ss.acc[l] : 0.0;
+    int gcur = ss.gcur;
+    bool first_group = ss.first_group != 0;
     for (int s = 0; s < nsrc; s++) {
-      const int gs = group_start(nsrc, nw, s);
-      if (s > 0 && gs != gcur) {
+      const int gs = group_start(nsrc_total, nw, s0 + s);
+      if (s0 + s > 0 && gs != gcur) {
         tot = first_group ? acc : tot + acc;
         first_group = false;
         acc = 0.0;
@@ -895,9 +918,17 @@ __global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int nw, long long
       }
       acc = acc + ap[s].lam[l];
     }
-    out[l] = first_group ? acc : tot + acc;
+    if (ss.final_chunk) {
+      out[l] = first_group ? acc : tot + acc;
+    } else {
+      ss.acc[l] = acc;
+      ss.tot[l] = tot;
+    }
   }
 }
+
+// The group state after sources s0 .. s0+nsrc-1 (the same steps as the sums, on the host).
+void sum_state_advance(SumState* ss, int nsrc, int s0, int nsrc_total, int nw);
 
 template <int ND>
 static cudaError_t launch_adj_solve(const AdjArgs& aa, int nsm, cudaStream_t st) {
@@ -918,15 +949,16 @@ using namespace eik;
 
 
 // Per-source misfits summed as the reference does: 0.5*m per source within a group, then
-// over the groups (eikmaingrad.jl:137-150, 241).
-__global__ void adj_misfit_kernel(const double* misf, int nsrc, int nw, double* out) {
+// over the groups (eikmaingrad.jl:137-150, 241); chunked like adj_sum_kernel.
+__global__ void adj_misfit_kernel(const double* misf, int nsrc, int s0, int nsrc_total, int nw, SumState ss,
+                                  double* out) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  double tot = 0.0, acc = 0.0;
-  int gcur = 0;
-  bool first_group = true;
+  double tot = ss.tot ? ss.tot[0] : 0.0, acc = ss.acc ? ss.acc[0] : 0.0;
+  int gcur = ss.gcur;
+  bool first_group = ss.first_group != 0;
   for (int s = 0; s < nsrc; s++) {
-    const int gs = group_start(nsrc, nw, s);
-    if (s > 0 && gs != gcur) {
+    const int gs = group_start(nsrc_total, nw, s0 + s);
+    if (s0 + s > 0 && gs != gcur) {
       tot = first_group ? acc : tot + acc;
       first_group = false;
       acc = 0.0;
@@ -934,10 +966,89 @@ __global__ void adj_misfit_kernel(const double* misf, int nsrc, int nw, double* 
     }
     acc += 0.5 * misf[s];
   }
-  *out = first_group ? acc : tot + acc;
+  if (ss.final_chunk) {
+    *out = first_group ? acc : tot + acc;
+  } else {
+    ss.acc[0] = acc;
+    ss.tot[0] = tot;
+  }
 }
 
 namespace eik {
+static int host_group_start(int nsrc, int nw, int s) {
+  if (nw <= 1) return 0;
+  if (nsrc < nw) return s;
+  const int dis = nsrc / nw, resto = nsrc % nw;
+  int start = 0;
+  for (int gi = 0; gi < nw; gi++) {
+    const int sz = dis + (gi < resto ? 1 : 0);
+    if (s < start + sz) return start;
+    start += sz;
+  }
+  return start;
+}
+
+void sum_state_advance(SumState* ss, int nsrc, int s0, int nsrc_total, int nw) {
+  for (int s = 0; s < nsrc; s++) {
+    const int gs = host_group_start(nsrc_total, nw, s0 + s);
+    if (s0 + s > 0 && gs != ss->gcur) {
+      ss->first_group = 0;
+      ss->gcur = gs;
+    }
+  }
+}
+}  // namespace eik
+
+namespace eik {
+
+void gradient_footprint(const Model& m, const eik_extra& ep, long long nrec, int32_t whichgrad,
+                        size_t* per_source, size_t* fixed) {
+  // the named buffers of forward_device, gradient_core and eik_gradient, per source and fixed
+  const int nd = m.g.nd;
+  const unsigned long long N = (unsigned long long)m.N;
+  const bool refine = ep.refinearoundsrc != 0;
+  unsigned long long win = 1, nfmax = 1;
+  for (int d = 0; d < nd; d++) {
+    win *= 2ull * ep.noderadius + 2;
+    nfmax *= (2ull * ep.noderadius + 1) * ep.downscalefactor + 1;
+  }
+  const unsigned long long seedcap = refine ? std::max<unsigned long long>(win, 8) : 8;
+  const unsigned long long nf = refine ? nfmax : 1;
+  unsigned long long per = sizeof(SrcOut) + seedcap * (4 + 8) + N * (8 + 1 + 8 + 1) + sizeof(CoarseProblem) +
+                           std::max<unsigned long long>(N, nf) * (4 + 8 + 1 + 8 + 8) + 5 * 8;
+  if (refine) per += nf * (8 + 1 + 1 + 4 + 4 + 1) + sizeof(CoarseProblem) + 8 * (4 + 8) + nf * (8 + 8 + 1) + 1;
+  per += N * (8 + 8ull * nd + 8) + 8 + seedcap * 4 * 8 + nd * 8 + (refine ? nf * (8 + 8ull * nd) : 16) +
+         sizeof(AdjProblem);
+  per += 3ull * nd * 8 + 8;  // coordinates, receiver offsets, source-location gradient
+  const bool smoothing = (whichgrad == 1 || whichgrad == 3) && ep.smoothgradkern > 0;
+  unsigned long long fix = N * 8 + (smoothing ? N * 8 : 0) + (unsigned long long)std::max<long long>(nrec, 1) *
+                                                                 (8ull * nd + 16) + 8192;
+  if (smoothing) {
+    unsigned long long k = 1;
+    for (int d = 0; d < nd; d++) k *= (unsigned long long)ep.smoothgradkern;
+    fix += 8 * k;
+  }
+  *per_source = (size_t)per;
+  *fixed = (size_t)fix;
+}
+
+// Sources per chunk of a gradient call under the context's budget (nsrc when one call fits).
+static long long gradient_chunk(eik_ctx* ctx, const Model& m, const eik_extra& ep, long long nsrc, long long nrec,
+                                int32_t whichgrad) {
+  size_t per = 0, fix = 0;
+  gradient_footprint(m, ep, nrec, whichgrad, &per, &fix);
+  const size_t budget = ctx->scratch.budget;
+  if (fix + per * (size_t)nsrc <= budget) return nsrc;
+  const size_t state = 3 * sizeof(double) * (size_t)m.N + 64;  // carried from chunk to chunk
+  if (budget < fix + state + per) return 0;
+  long long c = (long long)((budget - fix - state) / per);
+  // node-sources of one launch are numbered in 32 bits
+  unsigned long long nf = 1;
+  for (int d = 0; d < m.g.nd; d++) nf *= (2ull * ep.noderadius + 1) * ep.downscalefactor + 1;
+  const unsigned long long span = std::max<unsigned long long>((unsigned long long)m.N, ep.refinearoundsrc ? nf : 1);
+  c = std::min<long long>(c, (long long)(((1ull << 32) - 1) / span));
+  return std::max<long long>(1, std::min(c, nsrc));
+}
 
 int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichgrad, const eik_extra& ep) {
   if (whichgrad < 1 || whichgrad > 3)
@@ -958,7 +1069,7 @@ int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichg
 int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
                          const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
                          const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit,
-                         eik_stats* stats, GradTail* tail_out) {
+                         eik_stats* stats, GradTail* tail_out, GradChunk* chunk) {
   int rc = EIK_OK;
   cudaStream_t st = ctx->stream;
   Scratch& S = ctx->scratch;
@@ -1047,6 +1158,9 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   ta.refine = ep.refinearoundsrc;
   ta.whichgrad = whichgrad;
   ta.ngroups = ngroups;
+  ta.s0 = chunk ? chunk->s0 : 0;
+  ta.nsrc_total = chunk ? chunk->nsrc_total : (int)nsrc;
+  ta.prevbuf = (chunk && chunk->prev_valid) ? chunk->prevbuf : nullptr;
   ta.probs = dprobs;
   ta.ap = dap;
   ta.fb = dfb;
@@ -1066,8 +1180,21 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
     adj_carry_kernel<<<(int)nsrc, 64, 0, st>>>(ta, ep.radiussmoothgradsrc, carry);
     adj_srcnodes_kernel<<<(int)nsrc, 128, 0, st>>>(ta, carry);
     if (ep.radiussmoothgradsrc > 0) adj_smooth_kernel<<<(int)nsrc, 256, 0, st>>>(ta, ep.radiussmoothgradsrc);
-    if (d_gradvel) adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ngroups, N, smoothing ? gsum : d_gradvel);
-    if (smoothing) {
+    SumState ss;
+    ss.acc = chunk ? chunk->acc : nullptr;
+    ss.tot = chunk ? chunk->tot : nullptr;
+    ss.first_group = chunk ? chunk->first_group : 1;
+    ss.gcur = chunk ? chunk->gcur : 0;
+    ss.final_chunk = chunk ? (chunk->final_chunk ? 1 : 0) : 1;
+    if (d_gradvel)
+      adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ta.s0, ta.nsrc_total, ngroups, N, ss,
+                                                   smoothing ? gsum : d_gradvel);
+    if (chunk && !chunk->final_chunk) {
+      // the group buffer as this chunk leaves it: its last source's final field
+      CUDA_OK(ctx, cudaMemcpyAsync(chunk->prevbuf, lam + (nsrc - 1) * N, sizeof(double) * N, cudaMemcpyDeviceToDevice,
+                                   st));
+    }
+    if (smoothing && ss.final_chunk) {
       // weights from pageable memory: the copy has left the vector when cudaMemcpyAsync returns
       const std::vector<double> w = gaussian_weights((int)ep.smoothgradkern, nd);
       const void* w_src = stage_host(ctx, w.data(), sizeof(double) * w.size());
@@ -1076,7 +1203,24 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
       CUDA_OK(ctx, launch_smoothgrad(m.g, (int)ep.smoothgradkern, gw, gsum, d_gradvel, st));
     }
   }
-  if (d_misfit) adj_misfit_kernel<<<1, 1, 0, st>>>(misf, (int)nsrc, ngroups, d_misfit);
+  if (d_misfit) {
+    SumState ms;
+    ms.acc = chunk ? chunk->macc : nullptr;
+    ms.tot = chunk ? chunk->mtot : nullptr;
+    ms.first_group = chunk ? chunk->first_group : 1;
+    ms.gcur = chunk ? chunk->gcur : 0;
+    ms.final_chunk = chunk ? (chunk->final_chunk ? 1 : 0) : 1;
+    adj_misfit_kernel<<<1, 1, 0, st>>>(misf, (int)nsrc, ta.s0, ta.nsrc_total, ngroups, ms, d_misfit);
+  }
+  if (chunk) {
+    SumState adv;
+    adv.first_group = chunk->first_group;
+    adv.gcur = chunk->gcur;
+    sum_state_advance(&adv, (int)nsrc, chunk->s0, chunk->nsrc_total, ngroups);
+    chunk->first_group = adv.first_group;
+    chunk->gcur = adv.gcur;
+    chunk->prev_valid = true;
+  }
   if (d_gradsrc && whichgrad != 1)
     CUDA_OK(ctx, cudaMemcpyAsync(d_gradsrc, gsrc, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToDevice, st));
   CUDA_OK(ctx, cudaGetLastError());
@@ -1115,7 +1259,86 @@ int gradient_tail_stats(eik_ctx* ctx, GradTail& tail, eik_stats* stats) {
   return rc;
 }
 
+// A gradient call whose sources do not fit the budget in one pipeline: chunks of `chunk`
+// sources in order, each a full forward + adjoint pipeline, with the group buffer and the
+// ordered sums handed from chunk to chunk, so that the result is the one-call result bit
+// for bit (the reference's per-group buffer, eikmaingrad.jl:182-190, 242-246, and its
+// group sums, :137-150). The caller releases the scratch of earlier calls before it
+// allocates this call's inputs. Inputs and outputs are device pointers (gradvel N, gradsrc
+// nsrc x nd, misfit 1, each nullable).
+int gradient_chunked(eik_ctx* ctx, const Model& m, int64_t nsrc, long long chunk, const double* d_cs,
+                     const int64_t* rec_off, const double* d_rec, const double* d_po, const double* d_so,
+                     int32_t whichgrad, const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit,
+                     eik_stats* stats) {
+  cudaStream_t st = ctx->stream;
+  int rc = EIK_OK;
+  const long long N = m.N;
+  const int nd = m.g.nd;
+  double* state = (double*)ctx->scratch.get("chunk_state", sizeof(double) * (3 * (size_t)N + 4), &rc);
+  long long* d_off = (long long*)ctx->scratch.get("chunk_off", sizeof(long long) * (size_t)(chunk + 1), &rc);
+  if (!state || !d_off) return fail(ctx, rc ? rc : EIK_ERR_CUDA, "chunk state exceeds the HBM budget");
+  CUDA_OK(ctx, cudaMemsetAsync(state, 0, sizeof(double) * (3 * (size_t)N + 4), st));
+  GradChunk gc;
+  gc.nsrc_total = (int)nsrc;
+  gc.acc = state;
+  gc.tot = state + N;
+  gc.prevbuf = state + 2 * N;
+  gc.macc = state + 3 * N;
+  gc.mtot = state + 3 * N + 1;
+  eik_stats acc_stats;
+  std::memset(&acc_stats, 0, sizeof acc_stats);
+  std::vector<long long> off((size_t)chunk + 1);
+  for (long long c0 = 0; c0 < nsrc; c0 += chunk) {
+    const long long nloc = std::min(chunk, (long long)nsrc - c0);
+    gc.s0 = (int)c0;
+    gc.final_chunk = c0 + nloc >= nsrc;
+    for (long long s = 0; s <= nloc; s++) off[(size_t)s] = rec_off[c0 + s] - rec_off[c0];
+    CUDA_OK(ctx, cudaMemcpyAsync(d_off, off.data(), sizeof(long long) * (size_t)(nloc + 1), cudaMemcpyHostToDevice, st));
+    const long long r0 = rec_off[c0];
+    eik_stats cs;
+    std::memset(&cs, 0, sizeof cs);
+    rc = gradient_core(ctx, m, nloc, d_cs + c0 * nd, d_off, d_rec + r0 * nd, d_po + r0, d_so + r0, whichgrad, ep,
+                       d_gradvel, d_gradsrc ? d_gradsrc + c0 * nd : nullptr, d_misfit, &cs, nullptr, &gc);
+    if (rc) return rc;  // gradient_core drained the stream: `off` may be rewritten
+    acc_stats.warn_mask |= cs.warn_mask;
+    acc_stats.err_mask |= cs.err_mask;
+    acc_stats.tile_activations += cs.tile_activations;
+    acc_stats.node_evals += cs.node_evals;
+    acc_stats.fine_ms += cs.fine_ms;
+    acc_stats.solve_ms += cs.solve_ms;
+    acc_stats.adj_ms += cs.adj_ms;
+    acc_stats.adj_rounds = std::max(acc_stats.adj_rounds, cs.adj_rounds);
+    acc_stats.launches += cs.launches + 1;
+    acc_stats.fwd_rounds = std::max(acc_stats.fwd_rounds, cs.fwd_rounds);
+    acc_stats.fine_replays += cs.fine_replays;
+    for (int k = 0; k < 7; k++) acc_stats.fwd_visits[k] += cs.fwd_visits[k];
+    acc_stats.chunks += 1;
+  }
+  if (stats) {
+    const double dms = stats->device_ms;
+    *stats = acc_stats;
+    stats->device_ms = dms;
+  }
+  return EIK_OK;
+}
+
 }  // namespace eik
+
+extern "C" int eik_gradient_bytes(eik_ctx* ctx, eik_model_id model, int64_t nsrc, int64_t nrec, const eik_extra* ep_in,
+                                  int32_t whichgrad, uint64_t* bytes) {
+  if (!ctx || !bytes) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto it = ctx->models.find(model);
+  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  eik_extra ep;
+  if (ep_in) ep = *ep_in;
+  else eik_extra_defaults(&ep);
+  if (nsrc < 0 || nrec < 0) return fail(ctx, EIK_ERR_ASSERT, "nsrc >= 0, nrec >= 0");
+  size_t per = 0, fix = 0;
+  gradient_footprint(it->second, ep, nrec, whichgrad, &per, &fix);
+  *bytes = (uint64_t)(fix + per * (size_t)nsrc);
+  return EIK_OK;
+}
 
 extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
                             const int64_t* rec_off, const double* rec, const double* pickobs,
@@ -1146,27 +1369,40 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
                      ? fail(ctx, rc, "scratch '%s' exceeds the HBM budget", name)    \
                      : fail(ctx, rc, "cudaMalloc of scratch '%s' failed", name);
   double *d_cs, *d_rec, *d_po, *d_so, *d_gv, *d_gs, *d_m;
-  long long* d_off;
+  long long* d_off = nullptr;
+  const long long chunk = gradient_chunk(ctx, m, ep, nsrc, nrec, whichgrad);
+  if (chunk < 1) return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "one source does not fit the HBM budget");
+  if (chunk < nsrc) {
+    // split: the inputs and outputs are allocated after the release of earlier scratch
+    CUDA_OK(ctx, cudaStreamSynchronize(st));
+    S.release_all();
+  }
   GET(d_cs, double, "in_cs", nsrc * nd);
-  GET(d_off, long long, "in_off", nsrc + 1);
   GET(d_rec, double, "in_rec", std::max<long long>(nrec, 1) * nd);
   GET(d_po, double, "in_pickobs", std::max<long long>(nrec, 1));
   GET(d_so, double, "in_stdobs", std::max<long long>(nrec, 1));
   GET(d_gv, double, "out_gradvel", N);
   GET(d_gs, double, "out_gradsrc", nsrc * nd);
   GET(d_m, double, "out_misfit", 1);
+  if (chunk >= nsrc) {
+    GET(d_off, long long, "in_off", nsrc + 1);
+  }
 #undef GET
   cudaEventRecord(ctx->ev0, st);
   CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
-  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
+  if (d_off) CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
   if (nrec) {
     CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
     CUDA_OK(ctx, cudaMemcpyAsync(d_po, pickobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
     CUDA_OK(ctx, cudaMemcpyAsync(d_so, stdobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
   }
   const bool wantvel = whichgrad == 1 || whichgrad == 3, wantsrc = whichgrad != 1;
-  rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
-                     wantsrc ? d_gs : nullptr, d_m, stats, nullptr);
+  if (chunk < nsrc)
+    rc = gradient_chunked(ctx, m, nsrc, chunk, d_cs, rec_off, d_rec, d_po, d_so, whichgrad, ep,
+                          wantvel ? d_gv : nullptr, wantsrc ? d_gs : nullptr, d_m, stats);
+  else
+    rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
+                       wantsrc ? d_gs : nullptr, d_m, stats, nullptr);
   if (rc) return rc;
   double hm = 0.0;
   CUDA_OK(ctx, cudaMemcpyAsync(&hm, d_m, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1214,12 +1450,23 @@ extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsr
   CUDA_OK(ctx, cudaStreamSynchronize(st));
   rc = check_positions(ctx, m.g, nsrc, hcs.data(), rec_off, hrec.data());
   if (rc) return rc;
-  long long* d_off = (long long*)ctx->scratch.get("in_off", sizeof(long long) * (nsrc + 1), &rc);
-  if (!d_off) return fail(ctx, rc, "scratch allocation failed");
-  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
-  rc = gradient_core(ctx, m, nsrc, coordsrc_dev, d_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad, ep,
-                     (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
-                     misfit_dev, stats, nullptr);
+  const long long chunk = gradient_chunk(ctx, m, ep, nsrc, nrec, whichgrad);
+  if (chunk < 1) return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "one source does not fit the HBM budget");
+  if (chunk < nsrc) {
+    // split: the scratch of earlier calls is released (the inputs are the caller's memory)
+    CUDA_OK(ctx, cudaStreamSynchronize(st));
+    ctx->scratch.release_all();
+    rc = gradient_chunked(ctx, m, nsrc, chunk, coordsrc_dev, rec_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad,
+                          ep, (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
+                          misfit_dev, stats);
+  } else {
+    long long* d_off = (long long*)ctx->scratch.get("in_off", sizeof(long long) * (nsrc + 1), &rc);
+    if (!d_off) return fail(ctx, rc, "scratch allocation failed");
+    CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
+    rc = gradient_core(ctx, m, nsrc, coordsrc_dev, d_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad, ep,
+                       (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
+                       misfit_dev, stats, nullptr);
+  }
   if (rc) return rc;
   cudaEventRecord(ctx->ev1, st);
   CUDA_OK(ctx, cudaStreamSynchronize(st));

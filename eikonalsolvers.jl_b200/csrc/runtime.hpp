@@ -89,10 +89,32 @@ int gradient_tail_stats(eik_ctx* ctx, GradTail& tail, eik_stats* stats);
 int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichgrad, const eik_extra& ep);
 // Forward + adjoint + assembly for nsrc sources whose inputs are on the device; outputs
 // (each nullable) stay on the device. tail_out (nullable) receives what to read back.
+// One chunk of the sources of a gradient call that is split to fit the HBM budget: its place
+// in the call and the state handed from chunk to chunk (the ordered group sums of the field
+// and of the misfit, and the group buffer as the previous chunk left it). The sum state
+// arrays start at zero; first_group/gcur start at 1/0 and are advanced on the host.
+struct GradChunk {
+  int s0 = 0;            // index of the chunk's first source in the call
+  int nsrc_total = 0;
+  bool final_chunk = true;
+  double* acc = nullptr;  // N: current group's partial sum of the field
+  double* tot = nullptr;  // N: sum of the finished groups
+  double* macc = nullptr; // misfit: current group / finished groups
+  double* mtot = nullptr;
+  double* prevbuf = nullptr;  // N: final field of the previous chunk's last source
+  bool prev_valid = false;
+  int first_group = 1;
+  int gcur = 0;
+};
+// Device bytes one gradient call of nsrc sources takes from the context's scratch budget
+// (the named buffers the forward and adjoint stages allocate), and the fixed part that does
+// not grow with the sources.
+void gradient_footprint(const Model& m, const eik_extra& ep, long long nrec, int32_t whichgrad,
+                        size_t* per_source, size_t* fixed);
 int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
                   const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
                   const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit, eik_stats* stats,
-                  GradTail* tail_out);
+                  GradTail* tail_out, GradChunk* chunk = nullptr);
 
 }  // namespace eik
 

@@ -24,7 +24,7 @@ EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
             "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc",
             "eik_ctx_set_param", "eik_plan_gradient", "eik_plan_run", "eik_plan_destroy", "eik_tracerays",
-            "eik_traveltime_rays", "eik_selftest_wait"]
+            "eik_traveltime_rays", "eik_selftest_wait", "eik_gradient_bytes"]
 
 # eik_stats.warn_mask bits and the reference's @warn messages they stand for
 WARNINGS = {
@@ -73,7 +73,7 @@ class eik_stats(C.Structure):
                 ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
                 ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_rounds", C.c_uint64),
                 ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64),
-                ("fine_replays", C.c_uint64), ("fwd_visits", C.c_uint64 * 7)]
+                ("fine_replays", C.c_uint64), ("fwd_visits", C.c_uint64 * 7), ("chunks", C.c_uint64)]
 
 
 _lib = None
@@ -107,6 +107,9 @@ def load():
                                           C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
         L.eik_ttimemisfit_noalloc.argtypes = [C.POINTER(eik_grid), C.c_int64, P, P, P, P, P, P, P]
         L.eik_ttimemisfit_noalloc.restype = C.c_int
+        L.eik_gradient_bytes.argtypes = [P, C.c_int64, C.c_int64, C.c_int64, C.POINTER(eik_extra), C.c_int32,
+                                         C.POINTER(C.c_uint64)]
+        L.eik_gradient_bytes.restype = C.c_int
         L.eik_selftest_wait.argtypes = [P, C.c_double]
         L.eik_selftest_wait.restype = C.c_int
         L.eik_ctx_set_param.argtypes = [P, C.c_char_p, C.c_double]

@@ -48,6 +48,17 @@ class Context:
         """Scheduling parameter of this context (see eik_ctx_set_param)."""
         _lib.check(self.L.eik_ctx_set_param(self.h, name.encode(), float(value)), self.h)
 
+    def gradient_bytes(self, model: int, nsrc: int, nrec: int, whichgrad="gradvel", extraparams=None,
+                       nthreads: int = 1) -> int:
+        """Device bytes one gradient pipeline of nsrc sources and nrec receivers in all takes
+        from this context's budget (eik_gradient_bytes); larger calls are split into chunks."""
+        wg = whichgrad.lstrip(":") if isinstance(whichgrad, str) else whichgrad
+        ep = _lib.extra_struct(extraparams, nthreads)
+        out = C.c_uint64()
+        _lib.check(self.L.eik_gradient_bytes(self.h, C.c_int64(model), int(nsrc), int(nrec), C.byref(ep),
+                                             WHICHGRAD[wg], C.byref(out)), self.h)
+        return int(out.value)
+
     def selftest_wait(self, timeout_s: float = 0.2) -> int:
         """Runs one bounded device wait on a flag that nothing sets (eik_selftest_wait) and
         returns its status: EIK_ERR_TIMEOUT (-6) when the wait limit works."""

@@ -106,6 +106,7 @@ typedef struct {
   uint64_t fwd_visits[7];    /* forward list visits by outcome: value cached above the front,
                                 source point, nothing reached, bound above the front,
                                 evaluated above the front, evaluated unchanged, changed */
+  uint64_t chunks;           /* gradient calls split to fit the HBM budget: pipelines run (else 0) */
 } eik_stats;
 
 /* Fills the reference defaults of ExtraParams(). */
@@ -152,6 +153,13 @@ int eik_model_upload(eik_ctx* ctx, const eik_grid* grd, const double* vel, eik_m
 int eik_model_upload_device(eik_ctx* ctx, const eik_grid* grd, const double* vel_dev, eik_model_id* out);
 int eik_model_release(eik_ctx* ctx, eik_model_id model);
 
+/* No counterpart in the reference: device bytes that one eik_gradient pipeline of nsrc
+ * sources and nrec receivers in all takes from the context's HBM budget (the forward and
+ * adjoint state of every source plus the fixed part). A serving loop uses it for admission;
+ * eik_gradient splits a call whose footprint exceeds the budget. */
+int eik_gradient_bytes(eik_ctx* ctx, eik_model_id model, int64_t nsrc, int64_t nrec, const eik_extra* ep,
+                       int32_t whichgrad, uint64_t* bytes);
+
 /* Replaces ttforwsomesrc (eikmainfwd.jl:152-199) for all nsrc sources at once.
  * picks: rec_off[nsrc] values. ttgrids: nullable, nsrc x N traveltime grids (returntt). */
 int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
@@ -160,7 +168,12 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
 
 /* Replaces calcgradsomesrc (eikmaingrad.jl:174-258) with the sources in one group (the
  * :serial order). gradvel: nullable N values; gradsrc: nullable nsrc x ndim; misfit: the
- * summed 0.5*Σ(t-obs)²/σ² of the group. */
+ * summed 0.5*Σ(t-obs)²/σ² of the group. A call whose device footprint (eik_gradient_bytes)
+ * exceeds the context's HBM budget runs as several pipelines over consecutive chunks of its
+ * sources, recomputing each chunk's traveltimes instead of keeping all of them, with the
+ * gradient carried between sources (the reference's per-group buffer) and the ordered sums
+ * handed from chunk to chunk: the result is the one-pipeline result bit for bit
+ * (eik_stats.chunks gives the number of pipelines). */
 int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc,
                  const int64_t* rec_off, const double* rec, const double* pickobs,
                  const double* stdobs, int32_t whichgrad, const eik_extra* ep, double* gradvel,
