@@ -18,10 +18,17 @@ Lines printed by rank 0 (one JSON object):
             inside the timed region
   plain     the same workload one source per call (the unbatched path)
   roofline  HBM roofline of the dominant kernel (algorithmic bytes / measured duration)
-  cpu_baseline  the oracle (C++ restatement of the reference algorithm) on the host cores
+  cpu_baseline  the oracle (C++ restatement of the reference algorithm) on the host cores, on
+            the 256^3 workload itself (one source per thread), with the earlier 128^3
+            sub-block sample beside it
   serve     the serving leg: Poisson arrivals of a mixed traveltime/gradient workload
   rays      the ray-tracing leg (tracerays on 128^3 grids): GPU rays/s beside the oracle's
   hmc       HMC-style evaluations: eik_gradient per new velocity vs a replayed CUDA-graph plan
+  parity    the timed configuration against the oracle: forward fields of 4 of the batched
+            call's sources bit for bit, the gradient of the CPU leg's sources (rel. L2)
+  configs   the other benchmark configurations (2D 300x220 traveltime, 2D 1024x640 and
+            Grid3DSphere 200x180x180 gradients) end to end beside the oracle, and the batched
+            call over one source per call at 64^3, 128^3 and 512x320
 
 --impl reference: times the oracle on the host cores instead (rank 0 only).
 """
@@ -59,6 +66,9 @@ def parse():
     ap.add_argument("--plain-sources", type=int, default=2,
                     help="sources timed one per call for the plain path (0 = skip)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-parity", action="store_true", help="skip the parity check against the oracle")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other benchmark configurations and the batched/plain sizes")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--serve-requests", type=int, default=30,
                     help="requests of the serving leg (Poisson arrivals; 0 = skip)")
@@ -149,16 +159,17 @@ class Clocks:
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
 
 
-def host_cores(cap=32):
+def host_cores(cap=32, gb_per_thread=1.5):
     """Host threads for the CPU leg: all cores this process may use, at most `cap` and at
-    most one per 1.5 GB of available RAM (the oracle holds ~1 GB per 128^3 gradient)."""
+    most one per `gb_per_thread` GB of available RAM (the oracle holds ~1 GB per 128^3
+    gradient, ~10 GB per 256^3 gradient)."""
     try:
         n = len(os.sched_getaffinity(0))
     except AttributeError:
         n = os.cpu_count() or 1
     try:
         avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
-        n = min(n, max(1, int(avail / 1.5e9)))
+        n = min(n, max(1, int(avail / (gb_per_thread * 1e9))))
     except (ValueError, OSError):
         pass
     return max(1, min(n, cap))
@@ -227,7 +238,62 @@ def run_cpu_leg(w, steps, warmup, nthreads):
     sample = (f"{nsrc} sources (one per thread) of the workload on a {grd.grsize[0]}^3 sub-block of its "
               f"model, gradvelandsrcloc, {t:.2f} s per call; source-solves/s scaled to 256^3 by node count "
               f"(x{frac:.4g})")
-    return value, sample
+    return value, sample, t
+
+
+def run_cpu_full(w, nthreads, ep):
+    """The oracle on the benchmark workload itself (256^3): `nthreads` of its sources, one per
+    thread (:sharedmem, one source per group), :gradvelandsrcloc, timed once. Returns the
+    source-solves/s, a description, and the oracle's result with its inputs (the parity check
+    runs the GPU on the same inputs)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import eikoracle as O
+    k = max(1, min(nthreads, len(w.coordsrc)))
+    idx = list(range(k))
+    cs = w.coordsrc[idx]
+    rec = [w.coordrec[i] for i in idx]
+    po = [w.pickobs[i] for i in idx]
+    so = [w.stdobs[i] for i in idx]
+    t0 = time.perf_counter()
+    res = O.eikgradient(w.vel, w.grd, cs, rec, po, so, "gradvelandsrcloc", extraparams=ep, nthreads=k)
+    t = time.perf_counter() - t0
+    sample = (f"{k} sources of the {w.grd.grsize[0]}^3 workload itself, one per thread (:sharedmem), "
+              f":gradvelandsrcloc, {t:.1f} s for the call")
+    return k / t, sample, (cs, rec, po, so, k, res)
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+def run_parity(ctx, mid, w, ep, full, sel=(0, 7, 15, 31)):
+    """Parity of the benchmarked configuration against the oracle: the traveltime fields of
+    sources `sel` of one batched call over all the workload's sources (the timed call's
+    forward) bit for bit, and the gradient of the CPU leg's sources (same inputs, same
+    :sharedmem groups) within the gradient tolerance."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import eikoracle as O
+    from eikonalsolvers.tune import default_tuner
+    sel = [s for s in sel if s < len(w.coordsrc)]
+    default_tuner().apply_known(ctx, w.grd, len(w.coordsrc), ep)
+    _, tt = ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec, returntt=True, extraparams=ep)
+    _, ott = O.eiktraveltime(w.vel, w.grd, w.coordsrc[sel], [w.coordrec[i] for i in sel], returntt=True,
+                             extraparams=ep, nthreads=len(sel))
+    ndiff = [int((tt[s] != ott[k]).sum()) for k, s in enumerate(sel)]
+    del tt, ott
+    out = {"forward_sources_checked": sel, "forward_nodes_differing": ndiff,
+           "forward_bitexact": all(n == 0 for n in ndiff)}
+    if full is not None:
+        cs, rec, po, so, k, ores = full
+        from eikonalsolvers import ExtraParams
+        epg = ExtraParams(parallelkind="sharedmem")
+        default_tuner().apply_known(ctx, w.grd, k, epg)
+        gv, gs, m = ctx.gradient(mid, w.grd, cs, rec, po, so, "gradvelandsrcloc", extraparams=epg, nthreads=k)
+        out.update({"grad_sources": k, "gradvel_rel_l2": rel_l2(gv, ores[0]), "gradsrc_rel_l2": rel_l2(gs, ores[1]),
+                    "misfit_rel": abs(m - ores[2]) / abs(ores[2]), "grad_tolerance": 1e-4})
+    return out
 
 
 # ----------------------------------------------------------------------- GPU arm --
@@ -404,15 +470,28 @@ def main_b200(args):
             "share_of_step": kms / ms,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()}}
 
-    # ---- CPU baseline (rank 0, N=1 only)
+    # ---- CPU baseline (rank 0, N=1 only): the workload itself, and the 128^3 sub-block sample
     cpu = None
+    full = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cores = host_cores()
+        cores = host_cores(cap=32, gb_per_thread=10.0 * (args.scale ** 3))
         try:
-            v, sample = run_cpu_leg(w, steps=1, warmup=0, nthreads=cores)
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+            vf, samplef, full = run_cpu_full(w, cores, ExtraParams(parallelkind="sharedmem"))
+            cpu = {"value": vf, "unit": UNIT, "cores": full[4], "kind": "port", "sample": samplef}
         except Exception as e:  # the GPU line is still worth printing
             cpu = {"value": None, "unit": UNIT, "cores": cores, "kind": "port", "error": str(e)}
+        try:
+            cores_s = host_cores()
+            v, sample, _ = run_cpu_leg(w, steps=1, warmup=0, nthreads=cores_s)
+            cpu["subblock_sample"] = {"value": v, "cores": cores_s, "sample": sample}
+        except Exception as e:
+            cpu["subblock_sample"] = {"error": str(e)}
+    parity = None
+    if rank == 0 and ws == 1 and not args.no_parity:
+        try:
+            parity = run_parity(ctx, mid, w, ep, full)
+        except Exception as e:
+            parity = {"error": str(e)}
 
     if rank == 0:
         line = {
@@ -430,6 +509,7 @@ def main_b200(args):
             "plain": plain,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "parity": parity,
             "clocks": clocks,
             "gpu_launches": int(launches),
             "serve": None,
@@ -454,6 +534,11 @@ def main_b200(args):
                 line["rays"] = run_rays_leg(args, local)
             except Exception as e:
                 line["rays"] = {"error": str(e)}
+        if ws == 1 and not args.no_configs:
+            try:
+                line["configs"] = run_configs_leg(args, local)
+            except Exception as e:
+                line["configs"] = {"error": str(e)}
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.destroy_process_group()
@@ -582,16 +667,157 @@ def run_serve_leg(args, device):
     return st
 
 
+def _obs(ctx, w, vel, sigma, seed):
+    mid = ctx.upload(vel, w.grd)
+    try:
+        picks = ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec)
+    finally:
+        ctx.release(mid)
+    rng = np.random.default_rng(seed)
+    return [p + rng.normal(0.0, sigma, p.shape) for p in picks], [sigma * np.ones(p.shape) for p in picks]
+
+
+def _gpu_timed(fn, reps):
+    fn()  # warm-up: scratch growth, first-call set-up
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts))
+
+
+def run_configs_leg(args, device):
+    """The other benchmark configurations, each end to end through the host C-ABI entry point
+    (inputs and results in host memory, copies inside the host-clock timing) beside the oracle
+    on the host cores, with the roofline of the dominant kernel of the call; and the batched
+    call against one source per call at several grid sizes."""
+    from eikonalsolvers import Context, ExtraParams
+    from eikonalsolvers import configs as CF
+    from eikonalsolvers.tune import default_tuner
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import eikoracle as O
+    peak, peak_kind = measured_peaks()
+    cores = host_cores()
+    out = {}
+    ctx = Context(device)
+    try:
+        def leg(name, w, kind, ncpu, cpu_ep, desc):
+            nsrc = len(w.coordsrc)
+            N = int(np.prod(w.grd.grsize))
+            ep = ExtraParams()
+            if not default_tuner().apply_known(ctx, w.grd, nsrc, ep):
+                ctx.set_param("round_gate", 0.0)
+                ctx.set_param("ctas_per_sm", 0)
+            mid = ctx.upload(w.vel, w.grd)
+            try:
+                if kind == "traveltime":
+                    call = lambda: ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec, returntt=True, extraparams=ep)  # noqa: E731
+                else:
+                    call = lambda: ctx.gradient(mid, w.grd, w.coordsrc, w.coordrec, w.pickobs, w.stdobs, "gradvel",  # noqa: E731
+                                                extraparams=ep)
+                t = _gpu_timed(call, reps=3)
+                st = ctx.last_stats
+            finally:
+                ctx.release(mid)
+            k = max(1, min(ncpu, nsrc))
+            t0 = time.perf_counter()
+            if kind == "traveltime":
+                O.eiktraveltime(w.vel, w.grd, w.coordsrc[:k], w.coordrec[:k], returntt=True, extraparams=cpu_ep,
+                                nthreads=min(k, cores))
+            else:
+                O.eikgradient(w.vel, w.grd, w.coordsrc[:k], w.coordrec[:k], w.pickobs[:k], w.stdobs[:k], "gradvel",
+                              extraparams=cpu_ep, nthreads=min(k, cores))
+            tc = time.perf_counter() - t0
+            kern = {"coarse_rounds_kernel": float(st.solve_ms), "adj_rounds_kernel": float(st.adj_ms)}
+            top = max(kern, key=kern.get)
+            alg = 16 * N * nsrc
+            achieved = alg / (kern[top] / 1000.0) / 1e9 if kern[top] > 0 else None
+            out[name] = {"workload": desc, "gpu_e2e": {"value": nsrc / t, "unit": UNIT, "ms_per_call": t * 1e3,
+                                                       "device_ms": float(st.device_ms)},
+                         "cpu_baseline": {"value": k / tc, "unit": UNIT, "cores": min(k, cores), "kind": "port",
+                                          "sample": f"{k} of the sources, one per thread"},
+                         "gpu_over_cpu": (nsrc / t) / (k / tc),
+                         "roofline": {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak,
+                                      "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg,
+                                      "avg_launch_ms": kern[top]},
+                         "fwd_rounds": int(st.fwd_rounds)}
+            log(f"config {name}: GPU {nsrc / t:.1f} src/s, CPU {k / tc:.2f} src/s")
+
+        w1 = CF.cfg1()
+        leg("cfg1", w1, "traveltime", 4, ExtraParams(parallelkind="sharedmem"),
+            "2D Cartesian 300x220 h=0.5, v=2.5+0.034j, 4 sources x 10 receivers, eiktraveltime + returntt")
+        w2 = CF.cfg2()
+        w2.pickobs, w2.stdobs = _obs(ctx, w2, w2.vel_obs, 0.01, 11)
+        leg("cfg2", w2, "gradient", cores, ExtraParams(parallelkind="sharedmem"),
+            "2D Cartesian 1024x640 h=0.25, correlated random field 2-5, 64 sources x 200 receivers, :gradvel")
+        w4 = CF.cfg4()
+        w4.pickobs, w4.stdobs = _obs(ctx, w4, w4.vel, 0.05, 13)
+        leg("cfg4", w4, "gradient", cores, ExtraParams(parallelkind="sharedmem"),
+            "Grid3DSphere 200x180x180, r 5771-6371 km, 20x20 deg, 1D profile + 3% correlated, 48 sources x 500 "
+            "receivers, :gradvel")
+        # batched vs one source per call at several sizes (device-resident work, host clock)
+        bp = {}
+        for name, w, which, kplain in (("3D 64^3 x32", CF.cfg3(scale=0.25, nsrc=32), "gradvelandsrcloc", 4),
+                                       ("3D 128^3 x16", CF.cfg3(scale=0.5, nsrc=16), "gradvelandsrcloc", 2),
+                                       ("2D 512x320 x64", CF.cfg2(scale=0.5, nsrc=64), "gradvel", 4)):
+            nsrc = len(w.coordsrc)
+            w.pickobs, w.stdobs = _obs(ctx, w, w.vel * 1.03, 0.01, 5)
+            ep = ExtraParams()
+            mid = ctx.upload(w.vel, w.grd)
+            try:
+                def batched():
+                    if not default_tuner().apply_known(ctx, w.grd, nsrc, ep):
+                        ctx.set_param("round_gate", 0.0)
+                        ctx.set_param("ctas_per_sm", 0)
+                    ctx.gradient(mid, w.grd, w.coordsrc, w.coordrec, w.pickobs, w.stdobs, which, extraparams=ep)
+
+                def plain():
+                    if not default_tuner().apply_known(ctx, w.grd, 1, ep):
+                        ctx.set_param("round_gate", 0.0)
+                        ctx.set_param("ctas_per_sm", 0)
+                    for s in range(kplain):
+                        ctx.gradient(mid, w.grd, w.coordsrc[s:s + 1], w.coordrec[s:s + 1], w.pickobs[s:s + 1],
+                                     w.stdobs[s:s + 1], which, extraparams=ep)
+                tb = _gpu_timed(batched, reps=2)
+                tp = _gpu_timed(plain, reps=1)
+            finally:
+                ctx.release(mid)
+            bp[name] = {"batched": nsrc / tb, "plain": kplain / tp, "batched_over_plain": (nsrc / tb) / (kplain / tp),
+                        "unit": UNIT}
+            log(f"batched/plain {name}: {bp[name]['batched_over_plain']:.2f}")
+        out["batched_over_plain_by_size"] = bp
+    finally:
+        ctx.close()
+    return out
+
+
 def main_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
     cores = host_cores()
     w = make_workload(args.scale, args.nsrc)
-    v, sample = run_cpu_leg(w, steps=args.steps, warmup=args.warmup, nthreads=cores)
+    v, sample, t_step = run_cpu_leg(w, steps=args.steps, warmup=args.warmup, nthreads=cores)
+    # beside the bounded per-step sample: one call on the workload itself (one source per
+    # thread), with observations from straight rays at the model's mean velocity (the cost of
+    # the gradient does not depend on the observed values)
+    full = None
+    if not args.no_cpu:
+        from eikonalsolvers import ExtraParams
+        try:
+            vm = float(np.mean(w.vel))
+            w.pickobs = [np.linalg.norm(r - c[None, :], axis=1) / vm for c, r in zip(w.coordsrc, w.coordrec)]
+            w.stdobs = [0.01 * np.ones(p.shape) for p in w.pickobs]
+            fv, fsample, res = run_cpu_full(w, host_cores(cap=32, gb_per_thread=10.0 * (args.scale ** 3)),
+                                            ExtraParams(parallelkind="sharedmem"))
+            full = {"value": fv, "unit": UNIT, "cores": res[4], "kind": "port", "sample": fsample}
+        except Exception as e:
+            full = {"error": str(e)}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": f"3D Cartesian eikgradient :gradvelandsrcloc, {w.grd.grsize[0]}^3, "
                                    f"hgrid {w.grd.hgrid}, 4-layer model, {args.nsrc} sources per GPU, 400 receivers, "
                                    "default ExtraParams (refined start-up ds=5 r=3, smoothing radius 3)",
@@ -599,7 +825,8 @@ def main_reference(args):
                        "implementation": "oracle (C++ restatement of the reference FMM + CSR adjoint), "
                                          "threaded by source groups as :sharedmem; each step a bounded sample "
                                          "of the workload (see cpu_baseline.sample)"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                             "full_workload": full},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0

@@ -235,28 +235,40 @@ int err_to_rc(eik_ctx* ctx, uint32_t e) {
 }
 
 // -------------------------------------------------------------- forward pipeline --
-// Runs the start-up stage and the coarse solve for nsrc sources whose coordinates,
-// receiver offsets and receivers are already on the device. On return the traveltimes of
-// source s are at fw.t + s*N (codes at fw.code + s*N).
-int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const eik_extra& ep,
-                   ForwardState* fw, eik_stats* stats) {
+// Runs the start-up stage and the coarse solve for the sources of several models (nmod >= 1;
+// src_off[i]..src_off[i+1] are model i's sources, all models of one dimension) whose
+// coordinates are already on the device. The grids may differ in size: every source is a
+// problem with its own grid, numbered in the round solver with the largest grid's node
+// count as stride, so all of them share one persistent launch. The start-up stage runs per
+// model on its slice of the per-source arrays; the refined windows share one launch. On
+// return the traveltimes of source s are at fw.t + s*fw.N (its first npts of its model's
+// grid; codes at fw.code + s*fw.N).
+int forward_multi(eik_ctx* ctx, int nmod, const Model* const* models, const int64_t* src_off, const double* d_cs,
+                  const eik_extra& ep, ForwardState* fw, eik_stats* stats) {
   int rc = EIK_OK;
-  const GridDesc& g = m.g;
-  const long long N = m.N;
+  const int64_t nsrc = src_off[nmod];
+  const int nd = models[0]->g.nd;
+  long long N = 0;  // stride: the largest grid
+  unsigned long long work = 0;
+  for (int i = 0; i < nmod; i++) {
+    if (models[i]->g.nd != nd) return fail(ctx, EIK_ERR_ASSERT, "models of one call have one dimension");
+    N = std::max<long long>(N, models[i]->N);
+    work += (unsigned long long)(src_off[i + 1] - src_off[i]) * (unsigned long long)models[i]->N;
+  }
   cudaStream_t st = ctx->stream;
   Scratch& S = ctx->scratch;
   ForwardBatch fb;
   std::memset(&fb, 0, sizeof fb);
-  fb.g = g;
+  fb.g = models[0]->g;
   fb.nsrc = (int32_t)nsrc;
   fb.ds = ep.downscalefactor;
   fb.noderadius = ep.noderadius;
-  fb.vel = m.vel;
-  fb.slow = m.slow;
+  fb.vel = models[0]->vel;
+  fb.slow = models[0]->slow;
   fb.coordsrc = d_cs;
   const bool refine = ep.refinearoundsrc != 0;
   long long win = 1, nfmax = 1;
-  for (int d = 0; d < g.nd; d++) {
+  for (int d = 0; d < nd; d++) {
     win *= 2LL * ep.noderadius + 2;
     nfmax *= (2LL * ep.noderadius + 1) * ep.downscalefactor + 1;
   }
@@ -290,31 +302,24 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   GET(kL, double, "kL", nsrc * N);
   GET(kd, uint8_t, "kd", nsrc * N);
   std::vector<CoarseProblem> hp(nsrc);
-  for (int64_t s = 0; s < nsrc; s++) {
-    CoarseProblem& P = hp[s];
-    P.g = g;
-    P.slow = m.slow;
-    P.t = t + s * N;
-    P.code = code + s * N;
-    P.kL = kL + s * N;
-    P.kd = kd + s * N;
-    P.delta = P.incmin = 0.0;  // set on the device from the model's smallest slowness
-    uniform_coeffs(g, &P.c1u, &P.c2u);
-  }
-  // round width: about one node's traveltime at the largest velocity, times round_gate
-  double hmin;
-  {
-    double dh[3];
-    node_dh(g, 0, dh);
-    hmin = dh[0];
-    for (int a = 1; a < g.nd; a++) hmin = std::min(hmin, dh[a]);
-  }
+  for (int i = 0; i < nmod; i++)
+    for (int64_t s = src_off[i]; s < src_off[i + 1]; s++) {
+      CoarseProblem& P = hp[s];
+      P.g = models[i]->g;
+      P.slow = models[i]->slow;
+      P.t = t + s * N;
+      P.code = code + s * N;
+      P.kL = kL + s * N;
+      P.kd = kd + s * N;
+      P.delta = P.incmin = 0.0;  // set on the device from the model's smallest slowness
+      uniform_coeffs(P.g, &P.c1u, &P.c2u);
+    }
   CoarseProblem* dp;
   GET(dp, CoarseProblem, "probs", nsrc);
   SolveArgs sa;
   std::memset(&sa, 0, sizeof sa);
   sa.nprob = (int32_t)nsrc;
-  sa.nd = g.nd;
+  sa.nd = nd;
   unsigned long long* ctr;
   GET(ctr, unsigned long long, "solve_ctr", 16);
   sa.activations = ctr;
@@ -364,20 +369,61 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   const void* hp_src = stage_host(ctx, hp.data(), sizeof(CoarseProblem) * nsrc);
   if (!hp_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
   CUDA_OK(ctx, cudaMemcpyAsync(dp, hp_src, sizeof(CoarseProblem) * nsrc, cudaMemcpyHostToDevice, st));
-  const unsigned long long work = (unsigned long long)nsrc * (unsigned long long)N;
   const double gate = ctx->gate_for(work);
   const int sms = ctx->sms_for(work);
-  problem_scale_kernel<<<(int)((nsrc + 127) / 128), 128, 0, st>>>(dp, (int)nsrc, m.dstat + 2, gate, hmin,
-                                                                  g.nd);
+  // model i's slice of the per-source arrays, for the per-model start-up launches
+  auto slice = [&](int i) {
+    ForwardBatch f = fb;
+    const int64_t o = src_off[i];
+    f.g = models[i]->g;
+    f.vel = models[i]->vel;
+    f.slow = models[i]->slow;
+    f.nsrc = (int32_t)(src_off[i + 1] - o);
+    f.coordsrc = d_cs + o * nd;
+    f.out = fb.out + o;
+    f.seed_lin = fb.seed_lin + o * fb.seedcap;
+    f.seed_tt = fb.seed_tt + o * fb.seedcap;
+    if (refine) {
+      f.fine_tt = fb.fine_tt + o * fb.nfmax;
+      f.fine_status = fb.fine_status + o * fb.nfmax;
+      f.fine_code = fb.fine_code + o * fb.nfmax;
+      f.fine_idx = fb.fine_idx + o * fb.nfmax;
+      f.fine_order = fb.fine_order + o * fb.nfmax;
+      f.fine_onh = fb.fine_onh + o * fb.nfmax;
+    }
+    return f;
+  };
+  int nlaunch = 0;
+  // round widths: about one node's traveltime at the model's largest velocity, times round_gate
+  for (int i = 0; i < nmod; i++) {
+    const int64_t ni = src_off[i + 1] - src_off[i];
+    if (ni == 0) continue;
+    double dh[3];
+    node_dh(models[i]->g, 0, dh);
+    double hmin = dh[0];
+    for (int a = 1; a < nd; a++) hmin = std::min(hmin, dh[a]);
+    problem_scale_kernel<<<(int)((ni + 127) / 128), 128, 0, st>>>(dp + src_off[i], (int)ni, models[i]->dstat + 2,
+                                                                  gate, hmin, nd);
+    nlaunch += 1;
+  }
   CUDA_OK(ctx, cudaMemsetAsync(fb.err, 0, sizeof(uint32_t) * 4, st));
   CUDA_OK(ctx, cudaMemsetAsync(fb.out, 0, sizeof(SrcOut) * nsrc, st));
   if (!ctx->capturing) cudaEventRecord(ctx->evk[0], st);
-  int nlaunch = 6;  // round widths, start-up, init, round init, seeds, solve
   if (refine && ctx->fine_replay) {
-    launch_fine(fb, st);
+    for (int i = 0; i < nmod; i++)
+      if (src_off[i + 1] > src_off[i]) {
+        launch_fine(slice(i), st);
+        nlaunch += 1;
+      }
   } else if (refine) {
     // the windows as round-solver problems, then the heap's stop reconstructed from keys
-    launch_fine_setup(fb, fprobs, m.dstat + 2, gate, fseed_lin, fseed_tt, fslow, fkL, fkd, st);
+    for (int i = 0; i < nmod; i++) {
+      const int64_t o = src_off[i];
+      if (src_off[i + 1] == o) continue;
+      launch_fine_setup(slice(i), fprobs + o, models[i]->dstat + 2, gate, fseed_lin + o * 8, fseed_tt + o * 8,
+                        fslow + o * fb.nfmax, fkL + o * fb.nfmax, fkd + o * fb.nfmax, st);
+      nlaunch += 2;
+    }
     SolveArgs fsa = sa;
     fsa.probs = fprobs;
     fsa.rs.stride = (unsigned long long)fb.nfmax;
@@ -386,14 +432,23 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
     launch_rounds_init(fsa, st);
     launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
     CUDA_OK(ctx, launch_coarse_solve(fsa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
-    launch_fine_select(fb, fprobs, ftie, st);
-    // stops decided by exact ties: the heap is replayed for the flagged sources only, the
-    // flags staying on the device (no host round trip between the stages)
-    launch_fine_replay(fb, ftie, st);
+    nlaunch += 3;
+    for (int i = 0; i < nmod; i++) {
+      const int64_t o = src_off[i];
+      if (src_off[i + 1] == o) continue;
+      launch_fine_select(slice(i), fprobs + o, ftie + o, st);
+      // stops decided by exact ties: the heap is replayed for the flagged sources only, the
+      // flags staying on the device (no host round trip between the stages)
+      launch_fine_replay(slice(i), ftie + o, st);
+      nlaunch += 2;
+    }
     CUDA_OK(ctx, cudaGetLastError());
-    nlaunch += 7;
   } else {
-    launch_srcbox(fb, st);
+    for (int i = 0; i < nmod; i++)
+      if (src_off[i + 1] > src_off[i]) {
+        launch_srcbox(slice(i), st);
+        nlaunch += 1;
+      }
   }
   if (!ctx->capturing) cudaEventRecord(ctx->evk[1], st);
   CUDA_OK(ctx, cudaGetLastError());
@@ -403,6 +458,7 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   CUDA_OK(ctx, launch_coarse_solve(sa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
   if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
   CUDA_OK(ctx, cudaGetLastError());
+  nlaunch += 4;  // coarse init, round init, seeds, solve
   fw->fb = fb;
   fw->sa = sa;
   fw->t = t;
@@ -417,6 +473,13 @@ int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_c
   fw->sms = sms;
   if (stats) stats->launches += nlaunch;
   return EIK_OK;
+}
+
+int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const eik_extra& ep,
+                   ForwardState* fw, eik_stats* stats) {
+  const Model* mm = &m;
+  const int64_t off[2] = {0, nsrc};
+  return forward_multi(ctx, 1, &mm, off, d_cs, ep, fw, stats);
 }
 
 int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats) {
@@ -674,6 +737,94 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
   if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
   if (ttgrids)
     CUDA_OK(ctx, cudaMemcpyAsync(ttgrids, fw.t, sizeof(double) * nsrc * m.N, cudaMemcpyDeviceToHost, st));
+  cudaEventRecord(ctx->ev1, st);
+  rc = collect_forward_stats(ctx, &fw, stats);
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->device_ms = ms;
+  }
+  return rc;
+}
+
+int eik_traveltime_multi(eik_ctx* ctx, int64_t nmodel, const eik_model_id* model_ids, const int64_t* src_off,
+                         const double* coordsrc, const int64_t* rec_off, const double* rec, const eik_extra* ep_in,
+                         double* picks, double* ttgrids, eik_stats* stats) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  if (nmodel < 1 || !model_ids || !src_off) return fail(ctx, EIK_ERR_ASSERT, "nmodel >= 1 and NULL argument");
+  if (nmodel > (1 << 20)) return fail(ctx, EIK_ERR_ASSERT, "more than 2^20 models in one call");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  std::vector<const Model*> mods(nmodel);
+  for (int64_t i = 0; i < nmodel; i++) {
+    auto it = ctx->models.find(model_ids[i]);
+    if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model_ids[i]);
+    mods[i] = &it->second;
+    if (mods[i]->g.nd != mods[0]->g.nd) return fail(ctx, EIK_ERR_ASSERT, "models of one call have one dimension");
+  }
+  if (src_off[0] != 0) return fail(ctx, EIK_ERR_ASSERT, "src_off[0] must be 0");
+  for (int64_t i = 0; i < nmodel; i++)
+    if (src_off[i + 1] < src_off[i]) return fail(ctx, EIK_ERR_ASSERT, "src_off must be non-decreasing");
+  const int64_t nsrc = src_off[nmodel];
+  eik_extra ep;
+  if (ep_in) ep = *ep_in;
+  else eik_extra_defaults(&ep);
+  int rc = check_extra(ctx, &ep);
+  if (rc) return rc;
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  if (nsrc == 0) return EIK_OK;
+  if (!coordsrc || !rec_off || (!rec && rec_off[nsrc] > 0) || (!picks && rec_off[nsrc] > 0))
+    return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  if (rec_off[0] != 0) return fail(ctx, EIK_ERR_ASSERT, "rec_off[0] must be 0");
+  const int nd = mods[0]->g.nd;
+  // receiver offsets relative to each model's first receiver: model i's at rel[src_off[i] + i ...]
+  std::vector<int64_t> rel(nsrc + nmodel);
+  for (int64_t i = 0; i < nmodel; i++) {
+    const int64_t o = src_off[i], n = src_off[i + 1] - o;
+    for (int64_t s = 0; s <= n; s++) rel[o + i + s] = rec_off[o + s] - rec_off[o];
+    rc = check_positions(ctx, mods[i]->g, n, coordsrc + o * nd, rel.data() + o + i, rec ? rec + rec_off[o] * nd : rec);
+    if (rc) return rc;
+    if (n > 0)
+      for (int a = 0; a < nd; a++)
+        if (mods[i]->g.n[a] < 3) return fail(ctx, EIK_ERR_ERROR, "BoundsError: grid axis %d has fewer than 3 nodes", a);
+  }
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const long long nrec = rec_off[nsrc];
+  double* d_cs = (double*)ctx->scratch.get("in_cs", sizeof(double) * nsrc * nd, &rc);
+  long long* d_off = (long long*)ctx->scratch.get("in_off", sizeof(long long) * (nsrc + nmodel), &rc);
+  double* d_rec = (double*)ctx->scratch.get("in_rec", sizeof(double) * std::max<long long>(nrec, 1) * nd, &rc);
+  double* d_picks = (double*)ctx->scratch.get("out_picks", sizeof(double) * std::max<long long>(nrec, 1), &rc);
+  if (!d_cs || !d_off || !d_rec || !d_picks) return fail(ctx, rc, "scratch allocation failed");
+  const void* rel_src = stage_host(ctx, rel.data(), sizeof(int64_t) * rel.size());
+  if (!rel_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a staging copy failed");
+  cudaEventRecord(ctx->ev0, st);
+  CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rel_src, sizeof(int64_t) * rel.size(), cudaMemcpyHostToDevice, st));
+  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
+  ForwardState fw;
+  rc = forward_multi(ctx, (int)nmodel, mods.data(), src_off, d_cs, ep, &fw, stats);
+  if (rc) return rc;
+  for (int64_t i = 0; i < nmodel; i++) {
+    const int64_t o = src_off[i], n = src_off[i + 1] - o;
+    if (n == 0 || rec_off[o + n] == rec_off[o]) continue;
+    launch_picks(mods[i]->g, fw.t + o * fw.N, fw.N, (int)n, d_off + o + i, d_rec + rec_off[o] * nd,
+                 d_picks + rec_off[o], st);
+    if (stats) stats->launches += 1;
+  }
+  CUDA_OK(ctx, cudaGetLastError());
+  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
+  if (ttgrids) {
+    // each source's grid at its own size, one after another
+    double* dst = ttgrids;
+    for (int64_t i = 0; i < nmodel; i++) {
+      const int64_t o = src_off[i], n = src_off[i + 1] - o;
+      if (n == 0) continue;
+      const size_t w = sizeof(double) * (size_t)mods[i]->N;
+      CUDA_OK(ctx, cudaMemcpy2DAsync(dst, w, fw.t + o * fw.N, sizeof(double) * (size_t)fw.N, w, (size_t)n,
+                                     cudaMemcpyDeviceToHost, st));
+      dst += n * mods[i]->N;
+    }
+  }
   cudaEventRecord(ctx->ev1, st);
   rc = collect_forward_stats(ctx, &fw, stats);
   if (stats) {

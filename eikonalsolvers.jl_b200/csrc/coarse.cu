@@ -666,8 +666,9 @@ __global__ void picks_kernel(GridDesc g, const double* t, long long N, int nsrc,
 // ------------------------------------------------------------------ launchers --
 void launch_coarse_init(const CoarseProblem* hprobs, const CoarseProblem* dprobs, int nprob,
                         const ForwardBatch& fb, const SolveArgs& sa, cudaStream_t st) {
-  const long long N = npts(hprobs[0].g);
-  coarse_init_kernel<<<1184, 256, 0, st>>>(dprobs, nprob, N);
+  (void)hprobs;
+  // every problem's first stride nodes: its grid, and the padding up to the call's largest grid
+  coarse_init_kernel<<<1184, 256, 0, st>>>(dprobs, nprob, (long long)sa.rs.stride);
   rounds_init_kernel<<<296, 256, 0, st>>>(sa);
   launch_rounds_seed(sa, fb.seed_lin, fb.seed_tt, fb.out, false, fb.seedcap, st);
 }

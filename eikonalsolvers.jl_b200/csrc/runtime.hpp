@@ -64,6 +64,11 @@ int fail(eik_ctx* ctx, int code, const char* fmt, ...);
 int make_griddesc(eik_ctx* ctx, const eik_grid* g, GridDesc* out);
 int forward_device(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const eik_extra& ep,
                    ForwardState* fw, eik_stats* stats);
+// The forward of the sources of several models of one dimension (model i: sources
+// src_off[i]..src_off[i+1]) in one pipeline; fw->N is then the largest grid's node count,
+// the stride of the per-source arrays.
+int forward_multi(eik_ctx* ctx, int nmod, const Model* const* models, const int64_t* src_off, const double* d_cs,
+                  const eik_extra& ep, ForwardState* fw, eik_stats* stats);
 int collect_forward_stats(eik_ctx* ctx, ForwardState* fw, eik_stats* stats);
 int check_positions(eik_ctx* ctx, const GridDesc& g, int64_t nsrc, const double* cs, const int64_t* recoff,
                     const double* rec);

@@ -151,6 +151,60 @@ class Context:
             return out, [ttg[s * N:(s + 1) * N].reshape(grd.grsize, order="F").copy() for s in range(nsrc)]
         return out
 
+    def traveltime_multi(self, requests, returntt=False, extraparams=None):
+        """Traveltimes for several models of one dimension in one device pipeline
+        (eik_traveltime_multi): ``requests`` is a list of (model, grd, coordsrc, coordrec);
+        returns one result per request, each as ``traveltime`` returns it for that request
+        alone (bit-identical values)."""
+        assert len(requests) > 0, "at least one request"
+        ids, offs, css, recs_all, grds = [], [0], [], [], []
+        for model, grd, coordsrc, coordrec in requests:
+            cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+            if isinstance(coordrec, np.ndarray) and coordrec.dtype != object:
+                coordrec = [coordrec]
+            recs = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+            assert cs.shape[0] == len(recs), "size(coordsrc,1)==length(coordrec)"
+            ids.append(int(model))
+            offs.append(offs[-1] + cs.shape[0])
+            css.append(cs)
+            recs_all.extend(recs)
+            grds.append(grd)
+        nd = grds[0].ndim
+        assert all(g.ndim == nd for g in grds), "models of one call have one dimension"
+        ids = np.asarray(ids, dtype=np.int64)
+        offs = np.asarray(offs, dtype=np.int64)
+        cs = np.ascontiguousarray(np.concatenate(css, axis=0))
+        recoff = np.zeros(len(recs_all) + 1, dtype=np.int64)
+        for s, r in enumerate(recs_all):
+            recoff[s + 1] = recoff[s] + r.shape[0]
+        rec = np.ascontiguousarray(np.concatenate(recs_all, axis=0)) if recs_all else np.zeros((0, nd))
+        picks = np.zeros(max(int(recoff[-1]), 1), dtype=np.float64)
+        Ns = [int(np.prod(g.grsize)) for g in grds]
+        ttg = None
+        if returntt:
+            ttg = np.zeros(max(sum(N * (offs[i + 1] - offs[i]) for i, N in enumerate(Ns)), 1), dtype=np.float64)
+        ep = _lib.extra_struct(extraparams)
+        st = _lib.eik_stats()
+        rc = self.L.eik_traveltime_multi(self.h, C.c_int64(len(ids)), _lib.ptr(ids), _lib.ptr(offs), _lib.ptr(cs),
+                                         _lib.ptr(recoff), _lib.ptr(rec), C.byref(ep), _lib.ptr(picks),
+                                         _lib.ptr(ttg), C.byref(st))
+        self.last_stats = st
+        _lib.check(rc, self.h)
+        _warn(st)
+        out, base = [], 0
+        for i, g in enumerate(grds):
+            srcs = range(int(offs[i]), int(offs[i + 1]))
+            pk = [picks[recoff[s]:recoff[s + 1]].copy() for s in srcs]
+            if returntt:
+                N = Ns[i]
+                tts = [ttg[base + k * N:base + (k + 1) * N].reshape(g.grsize, order="F").copy()
+                       for k in range(len(srcs))]
+                base += N * len(srcs)
+                out.append((pk, tts))
+            else:
+                out.append(pk)
+        return out
+
     def gradient(self, model: int, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad, extraparams=None,
                  nthreads: int = 1):
         """Misfit gradient for all sources in one batched device call.

@@ -166,6 +166,18 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
                    const int64_t* rec_off, const double* rec, const eik_extra* ep, double* picks,
                    double* ttgrids, eik_stats* stats);
 
+/* No counterpart in the reference as one call: ttforwsomesrc (eikmainfwd.jl:152-199) for the
+ * sources of several models of one dimension, whose grids may differ in size, in one
+ * pipeline (one persistent solve for all of them). Model model_ids[i] takes sources
+ * src_off[i]..src_off[i+1]-1 (src_off[0] = 0, non-decreasing, nmodel+1 values); coordsrc,
+ * rec_off (rec_off[0] = 0), rec and picks run over all sources in that order, as in
+ * eik_traveltime. ttgrids: nullable, each source's grid at its own model's node count, one
+ * after another. Every source's results are bit-identical to eik_traveltime of its model
+ * alone. */
+int eik_traveltime_multi(eik_ctx* ctx, int64_t nmodel, const eik_model_id* model_ids, const int64_t* src_off,
+                         const double* coordsrc, const int64_t* rec_off, const double* rec, const eik_extra* ep,
+                         double* picks, double* ttgrids, eik_stats* stats);
+
 /* Replaces calcgradsomesrc (eikmaingrad.jl:174-258) with the sources in one group (the
  * :serial order). gradvel: nullable N values; gradsrc: nullable nsrc x ndim; misfit: the
  * summed 0.5*Σ(t-obs)²/σ² of the group. A call whose device footprint (eik_gradient_bytes)
