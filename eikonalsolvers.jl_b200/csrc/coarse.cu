@@ -157,6 +157,12 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long* p, double v) 
 // One listed node: gate, evaluate, write back. Returns the directions of the nodes to list
 // for the next round (bit DIR_SELF: this node again) and, in *front, the traveltime that
 // bounds their next evaluation from below.
+//
+// The visit is a chain of dependent L2 round trips, which sets the length of a round when
+// fronts are small. Each stage therefore issues all of its loads before it uses any: the
+// node's own state, its immediate neighbours, their codes with the distance-2 nodes, and
+// the relist filter's reads per axis. Reordering these reads does not change what they
+// can observe (see the notes at each stage).
 template <int ND>
 __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, unsigned long long gbase, long long l,
                                  double T, int r, double* front, unsigned long long* evals,
@@ -164,17 +170,18 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   PL_T(tq0);
   const GridDesc& g = P.g;
   const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
-  // last evaluated value, still valid while nothing the node reads has changed
-  if (!__ldcg(a.rs.dirty + gbase + l)) {
-    const double tv = __ldcg(a.rs.tent + gbase + l);
-    if (tv > T && tv < EIK_INF) {
-      *front = tv;
-      vk[0]++;
-      return 1u << DIR_SELF;
-    }
-  }
+  // The node's own state in one batch. Only this visit writes its t, code and key during
+  // the round (a node is listed once per round), so their order of reading is free.
+  const uint8_t dirty0 = __ldcg(a.rs.dirty + gbase + l);
+  const double tv = __ldcg(a.rs.tent + gbase + l);
   const uint8_t cb = __ldcg(P.code + l);
   const double told = __ldcg(P.t + l);
+  // last evaluated value, still valid while nothing the node reads has changed
+  if (!dirty0 && tv > T && tv < EIK_INF) {
+    *front = tv;
+    vk[0]++;
+    return 1u << DIR_SELF;
+  }
   double Lold;
   int dold;
   node_key(P, l, told, cb, &Lold, &dold);
@@ -186,24 +193,30 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   // marks it dirty again (writers store the value, fence, then the flag)
   a.rs.dirty[gbase + l] = 0;
   __threadfence();
-  // immediate neighbours: potential (the smallest of their traveltimes)
+  // immediate neighbours (one batch with the slowness): potential = smallest traveltime
   double t1[ND][2];
   long long l1[ND][2];
-  double pot = EIK_INF;
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
     for (int s = 0; s < 2; s++) {
       const int sh = s == 0 ? 1 : -1;
       l1[ax][s] = -1;
-      t1[ax][s] = EIK_INF;
       if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
       int p[3] = {c[0], c[1], c[2]};
       p[ax] += sh;
       l1[ax][s] = lin3(g, p[0], p[1], p[2]);
-      t1[ax][s] = __ldcg(P.t + l1[ax][s]);
-      pot = fmin(pot, t1[ax][s]);
     }
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) t1[ax][s] = l1[ax][s] >= 0 ? __ldcg(P.t + l1[ax][s]) : EIK_INF;
+  const double slow = __ldg(P.slow + l);
+  double pot = EIK_INF;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) pot = fmin(pot, t1[ax][s]);
   if (!(pot < EIK_INF)) {  // nothing reached around it yet
     a.rs.tent[gbase + l] = EIK_INF;
     vk[2]++;
@@ -214,7 +227,7 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   Nbhd nb;
   nb_clear(nb);
   node_dh(g, c[0], nb.dh);
-  nb.slow = __ldg(P.slow + l);
+  nb.slow = slow;
   nb.c1u = P.c1u;
   nb.c2u = P.c2u;
   // Lower bound of the node's value: every term of the local update is at least pot and
@@ -230,16 +243,19 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
     vk[3]++;
     return 1u << DIR_SELF;
   }
+  // Codes of the immediate neighbours and the distance-2 nodes with their codes, one batch.
+  // A neighbour's key is read after its traveltime here as in any order: the key changes
+  // only together with the traveltime, in the neighbour's own visit.
+  uint8_t cd1[ND][2], cd2[ND][2];
+  double t2[ND][2];
+  long long l2[ND][2];
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-      if (l1[ax][s] < 0) continue;
       const int sh = s == 0 ? 1 : -1;
-      double L;
-      int d;
-      node_key(P, l1[ax][s], t1[ax][s], __ldcg(P.code + l1[ax][s]), &L, &d);
-      nb_put1(nb, ax, s, t1[ax][s], L, d);
+      l2[ax][s] = -1;
+      if (l1[ax][s] < 0) continue;
       int p[3] = {c[0], c[1], c[2]};
       p[ax] += sh;
       bool ok = true;  // isonbord on the first neighbour, in every coordinate (eikutils.jl:129-162)
@@ -248,10 +264,29 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
         if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
       if (ok) {
         p[ax] += sh;
-        const long long l2 = lin3(g, p[0], p[1], p[2]);
-        const double t2 = __ldcg(P.t + l2);
-        node_key(P, l2, t2, __ldcg(P.code + l2), &L, &d);
-        nb_put2(nb, ax, s, t2, L, d);
+        l2[ax][s] = lin3(g, p[0], p[1], p[2]);
+      }
+    }
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      cd1[ax][s] = l1[ax][s] >= 0 ? __ldcg(P.code + l1[ax][s]) : (uint8_t)0;
+      t2[ax][s] = l2[ax][s] >= 0 ? __ldcg(P.t + l2[ax][s]) : EIK_INF;
+      cd2[ax][s] = l2[ax][s] >= 0 ? __ldcg(P.code + l2[ax][s]) : (uint8_t)0;
+    }
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      if (l1[ax][s] < 0) continue;
+      double L;
+      int d;
+      node_key(P, l1[ax][s], t1[ax][s], cd1[ax][s], &L, &d);
+      nb_put1(nb, ax, s, t1[ax][s], L, d);
+      if (l2[ax][s] >= 0) {
+        node_key(P, l2[ax][s], t2[ax][s], cd2[ax][s], &L, &d);
+        nb_put2(nb, ax, s, t2[ax][s], L, d);
       }
     }
   int8_t cd[3] = {0, 0, 0};
@@ -289,33 +324,54 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
   // except those whose stored key is at most both the old and the new key of this node:
   // the order rule of such a node never accepts this one, nor is its termination test
   // affected, so its value cannot change. A node listed for the current round may be
-  // under evaluation right now and is always listed again.
+  // under evaluation right now and is always listed again. The node two steps away reads
+  // this one only through the node in between, which must be reached first; when it is,
+  // its own change lists that node.
+  //
+  // Reads per axis in one batch, all after the fence above: the in-between node's
+  // traveltime (the +-1 node's, read fresh), and the stamp, traveltime and code of each
+  // candidate. A candidate whose stamp is below r is in no list of this round, so nothing
+  // writes its traveltime, code or key while this round runs: reading them before or after
+  // the stamp observes the same values.
   const Key kold = Key{Lold, dold, told};
   unsigned dirs = 0;
 #pragma unroll
-  for (int k = 0; k < 4 * ND; k++) {
-    const int ax = k >> 2, off = dir_off(k);
-    if (c[ax] + off < 0 || c[ax] + off >= g.n[ax]) continue;
-    int p[3] = {c[0], c[1], c[2]};
-    p[ax] += off;
-    const long long lj = lin3(g, p[0], p[1], p[2]);
-    if (off == 2 || off == -2) {
-      // the node two steps away reads this one only through the node in between, which
-      // must be reached first; when it is, its own change lists that node
-      int m[3] = {c[0], c[1], c[2]};
-      m[ax] += off / 2;
-      if (!(__ldcg(P.t + lin3(g, m[0], m[1], m[2])) < EIK_INF)) continue;
+  for (int ax = 0; ax < ND; ax++) {
+    long long lj[4];
+    double tj[4];
+    uint8_t cj[4];
+    int32_t sj[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int off = dir_off(j);
+      lj[j] = -1;
+      if (c[ax] + off < 0 || c[ax] + off >= g.n[ax]) continue;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += off;
+      lj[j] = lin3(g, p[0], p[1], p[2]);
     }
-    if (*(volatile int32_t*)(a.rs.stamp + gbase + lj) < r) {
-      const double tj = __ldcg(P.t + lj);
-      double Lj;
-      int dj;
-      node_key(P, lj, tj, __ldcg(P.code + lj), &Lj, &dj);
-      const Key kj = Key{Lj, dj, tj};
-      if (key_le(kj, kold) && key_le(kj, nk)) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      tj[j] = lj[j] >= 0 ? __ldcg(P.t + lj[j]) : EIK_INF;
+      cj[j] = lj[j] >= 0 ? __ldcg(P.code + lj[j]) : (uint8_t)0;
+      sj[j] = lj[j] >= 0 ? *(volatile const int32_t*)(a.rs.stamp + gbase + lj[j]) : 0;
     }
-    a.rs.dirty[gbase + lj] = 1;
-    dirs |= 1u << k;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (lj[j] < 0) continue;
+      // j = 0 (-2) reads this node through j = 1 (-1), j = 3 (+2) through j = 2 (+1)
+      if (j == 0 && !(tj[1] < EIK_INF)) continue;
+      if (j == 3 && !(tj[2] < EIK_INF)) continue;
+      if (sj[j] < r) {
+        double Lj;
+        int dj;
+        node_key(P, lj[j], tj[j], cj[j], &Lj, &dj);
+        const Key kj = Key{Lj, dj, tj[j]};
+        if (key_le(kj, kold) && key_le(kj, nk)) continue;
+      }
+      a.rs.dirty[gbase + lj[j]] = 1;
+      dirs |= 1u << (4 * ax + j);
+    }
   }
   *front = nv + P.incmin;  // no node reading this one can get a smaller value from it
   PL_ADD(10, tq3);
@@ -398,9 +454,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
             const double ef = (double)__uint_as_float((unsigned int)e);
             prob = (int)(gid / N);
             l = (long long)(gid - (unsigned long long)prob * N);
-            const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) +
-                                                      a.probs[prob].delta);
-            if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
+            // threshold inputs and the dirty flag in one batch
+            const double tp = __ldcg(thr_prev + prob);
+            const unsigned long long nmv = ld_volatile(nm + prob);
+            const double del = a.probs[prob].delta;
+            const uint8_t dq = __ldcg(a.rs.dirty + gid);
+            const double T = fmax(tp, __longlong_as_double((long long)nmv) + del);
+            if (ef > T && ef < EIK_INF && !dq) {
               front = ef;
               dirs = 1u << DIR_SELF;
               vk[0]++;
@@ -509,9 +569,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_round
           l = (long long)(gid - (unsigned long long)prob * N);
           const CoarseProblem& P = a.probs[prob];
           // window of one round width above the smallest pending front, never moving back
-          const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
+          // (its inputs and the dirty flag in one batch)
+          const double tp = __ldcg(thr_prev + prob);
+          const unsigned long long nmv = ld_volatile(nm + prob);
+          const double del = P.delta;
+          const uint8_t dq = __ldcg(a.rs.dirty + gid);
+          const double T = fmax(tp, __longlong_as_double((long long)nmv) + del);
           const unsigned long long gb = (unsigned long long)prob * N;
-          if (ef > T && ef < EIK_INF && !__ldcg(a.rs.dirty + gid)) {
+          if (ef > T && ef < EIK_INF && !dq) {
             // still waiting and nothing it reads has changed: its front stands
             front = ef;
             dirs = 1u << DIR_SELF;
