@@ -78,6 +78,12 @@ def parse():
     ap.add_argument("--hmc-evals", type=int, default=20, help="evaluations of the HMC-style leg (0 = skip)")
     ap.add_argument("--ray-cpu-rays", type=int, default=24, help="rays the oracle traces for the CPU figure")
     ap.add_argument("--serve-scale", type=float, default=1.0, help="grid scale of the serving mix")
+    ap.add_argument("--serve-sweep", type=str, default="",
+                    help="comma-separated arrival rates (req/s): run only the serving sweep, each rate for "
+                         "min(2000, 60 s x rate) requests, and print one JSON line")
+    ap.add_argument("--serve-max-queue", type=int, default=64,
+                    help="waiting requests beyond which the sweep's server refuses arrivals")
+    ap.add_argument("--serve-batch-sources", type=int, default=128, help="source cap of a merged call")
     return ap.parse_args()
 
 
@@ -313,6 +319,10 @@ def main_b200(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
+    if args.serve_sweep:
+        if rank == 0:
+            print(json.dumps(run_serve_sweep(args, local)), flush=True)
+        return 0
     ctx = Context(local)
     L = ctx.L
 
@@ -632,14 +642,20 @@ def run_hmc_leg(args, device):
             "timing": "host clock per evaluation (median), velocity upload included"}
 
 
-def run_serve_leg(args, device):
+def run_serve_leg(args, device, rate=None, n=None, max_queue=0):
     """Serving mix (2D/3D Cartesian models resident on the device, 70 % traveltime / 30 %
     gradient requests with 1-64 sources) arriving as a Poisson process; latency from
-    submission to result, on the host clock."""
+    submission to result, on the host clock. A server with max_queue > 0 refuses arrivals
+    while that many requests wait (counted in `refused`)."""
     from eikonalsolvers import configs as CF
     from eikonalsolvers.serve import Request, Server
-    models, reqs = CF.serving_requests(n=args.serve_requests, rate=args.serve_rate, seed=9, scale=args.serve_scale)
-    with Server(device=device, slots=args.serve_slots) as srv:
+    rate = args.serve_rate if rate is None else rate
+    n = args.serve_requests if n is None else n
+    models, reqs = CF.serving_requests(n=n, rate=rate, seed=9, scale=args.serve_scale)
+    # server-wide admission: merged calls in flight together within 150 GB of device memory
+    with Server(device=device, slots=args.serve_slots, max_batch_sources=args.serve_batch_sources,
+                hbm_budget=150 * 10 ** 9, hbm_budget_per_slot=int(160e9 / args.serve_slots),
+                max_queue=max_queue) as srv:
         for k, (vel, grd, _) in models.items():
             srv.register_model(k, vel, grd)
         # warm each slot on every model (uploads, scratch growth) before the clock starts
@@ -658,13 +674,36 @@ def run_serve_leg(args, device):
             futs.append(srv.submit(Request(model=r["model"], kind=r["kind"], coordsrc=r["coordsrc"],
                                            coordrec=r["coordrec"], pickobs=r.get("pickobs"),
                                            stdobs=r.get("stdobs"))))
+        t_arrivals = time.perf_counter() - t0
+        failed = 0
         for f in futs:
-            f.result()
+            try:
+                f.result()
+            except Exception as e:
+                if type(e).__name__ != "ServerOverloaded":
+                    failed += 1
         st = srv.stats()
-    st.update({"offered_rate_req_s": args.serve_rate, "slots": args.serve_slots,
-               "mix": "seeded: 60% 2D side 128-1024, 40% 3D side 64-192, 1-64 sources, 70% traveltime / "
-                      "30% gradvel, 6 resident models"})
+    st.update({"offered_rate_req_s": rate, "offered_requests": n, "arrival_window_s": t_arrivals,
+               "failed": failed, "slots": args.serve_slots, "max_queue": max_queue,
+               "max_batch_sources": args.serve_batch_sources,
+               "mix": "seeded: 60% 2D side 128-1024, 40% 3D side 64-192 (x serve-scale), 1-64 sources, 70% "
+                      "traveltime / 30% gradvel, 6 resident models"})
     return st
+
+
+def run_serve_sweep(args, device):
+    rates = [float(x) for x in args.serve_sweep.split(",") if x.strip()]
+    out = []
+    for rate in rates:
+        n = int(min(2000, round(60.0 * rate)))
+        st = run_serve_leg(args, device, rate=rate, n=n, max_queue=args.serve_max_queue)
+        log(f"serve rate {rate}: {json.dumps(st)}")
+        out.append(st)
+    served = [(r["offered_rate_req_s"], r.get("requests_per_s") or 0.0) for r in out]
+    # saturation: the first rate whose served rate falls below 90 % of the offered one
+    sat = next((o for o, v in served if v < 0.9 * o), None)
+    return {"serve_sweep": out, "saturation_offered_rate_req_s": sat,
+            "served_rate_at_saturation_req_s": max(v for _, v in served) if served else None}
 
 
 def _obs(ctx, w, vel, sigma, seed):

@@ -385,7 +385,7 @@ struct SrcTermArgs {
   int nsrc;
   int refine;
   int whichgrad;
-  int ngroups;          // consecutive source groups with their own gradient buffer
+  const int32_t* gstart;  // per source of the whole call: first source of its group (own gradient buffer)
   int s0;               // index, in the whole call, of this chunk's first source
   int nsrc_total;       // sources of the whole call (groups are those of the whole call)
   const double* prevbuf;  // N: the group buffer before this chunk (its previous source's final field), or null
@@ -805,20 +805,6 @@ __device__ double smooth_factor(const GridDesc& g, const double* src, int R, int
   return (r <= rmax) ? r / rmax : 1.0;
 }
 
-// Source groups (distribsrcs, eikutils.jl:171-190): first source of the group of s.
-__device__ int group_start(int nsrc, int nw, int s) {
-  if (nw <= 1) return 0;
-  if (nsrc < nw) return s;
-  const int dis = nsrc / nw, resto = nsrc % nw;
-  int start = 0;
-  for (int gi = 0; gi < nw; gi++) {
-    const int sz = dis + (gi < resto ? 1 : 0);
-    if (s < start + sz) return start;
-    start += sz;
-  }
-  return start;
-}
-
 // The reference keeps one gradient buffer per source group and assigns only off the
 // current source's points (eikmaingrad.jl:182, 417-479), so a source point starts from
 // the previous source's smoothed value there. The carried value is a short recurrence over
@@ -832,7 +818,7 @@ __global__ void adj_carry_kernel(SrcTermArgs sa, int R, double* carry) {
   const int s = blockIdx.x;
   const ForwardBatch& fb = *sa.fb;
   const GridDesc& g = sa.g;
-  const int gs = group_start(sa.nsrc_total, sa.ngroups, sa.s0 + s) - sa.s0;  // < 0: began in an earlier chunk
+  const int gs = sa.gstart[sa.s0 + s] - sa.s0;  // < 0: began in an earlier chunk
   const int lo = gs > 0 ? gs : 0;
   for (int k = threadIdx.x; k < fb.out[s].nseeds; k += blockDim.x) {
     const long long l = fb.seed_lin[(size_t)s * fb.seedcap + k];
@@ -900,26 +886,31 @@ struct SumState {
 };
 
 // Σ over sources in the reference's order: within a group in source order, then the
-// group sums in group order (eikmaingrad.jl:137-150). Sources s0 .. s0+nsrc-1 of a call of
-// nsrc_total; the last chunk writes the total.
-__global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int s0, int nsrc_total, int nw, long long N,
-                               SumState ss, double* out) {
+// group sums in group order (eikmaingrad.jl:137-150). Sources s0 .. s0+nsrc-1 of a call;
+// gstart gives each source's group, the last chunk writes the total. With per-group
+// outputs (one chunk) each group's sum goes to out + (its ordinal) * N instead, as a call of
+// that group alone computes it.
+__global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int s0, const int32_t* gstart, int per_group,
+                               long long N, SumState ss, double* out) {
   for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < N; l += (long long)gridDim.x * blockDim.x) {
     double tot = ss.tot ? ss.tot[l] : 0.0, acc = ss.acc ? ss.acc[l] : 0.0;
-    int gcur = ss.gcur;
+    int gcur = ss.gcur, gord = 0;
     bool first_group = ss.first_group != 0;
     for (int s = 0; s < nsrc; s++) {
-      const int gs = group_start(nsrc_total, nw, s0 + s);
+      const int gs = gstart[s0 + s];
       if (s0 + s > 0 && gs != gcur) {
-        tot = first_group ? acc : tot + acc;
+        if (per_group) out[(size_t)gord * N + l] = acc;
+        else tot = first_group ? acc : tot + acc;
         first_group = false;
         acc = 0.0;
         gcur = gs;
+        gord++;
       }
       acc = acc + ap[s].lam[l];
     }
     if (ss.final_chunk) {
-      out[l] = first_group ? acc : tot + acc;
+      if (per_group) out[(size_t)gord * N + l] = acc;
+      else out[l] = first_group ? acc : tot + acc;
     } else {
       ss.acc[l] = acc;
       ss.tot[l] = tot;
@@ -928,7 +919,7 @@ __global__ void adj_sum_kernel(const AdjProblem* ap, int nsrc, int s0, int nsrc_
 }
 
 // The group state after sources s0 .. s0+nsrc-1 (the same steps as the sums, on the host).
-void sum_state_advance(SumState* ss, int nsrc, int s0, int nsrc_total, int nw);
+void sum_state_advance(SumState* ss, int nsrc, int s0, const int32_t* gstart);
 
 template <int ND>
 static cudaError_t launch_adj_solve(const AdjArgs& aa, int nsm, cudaStream_t st) {
@@ -949,25 +940,29 @@ using namespace eik;
 
 
 // Per-source misfits summed as the reference does: 0.5*m per source within a group, then
-// over the groups (eikmaingrad.jl:137-150, 241); chunked like adj_sum_kernel.
-__global__ void adj_misfit_kernel(const double* misf, int nsrc, int s0, int nsrc_total, int nw, SumState ss,
-                                  double* out) {
+// over the groups (eikmaingrad.jl:137-150, 241); chunked like adj_sum_kernel, per group
+// like it with per_group.
+__global__ void adj_misfit_kernel(const double* misf, int nsrc, int s0, const int32_t* gstart, int per_group,
+                                  SumState ss, double* out) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   double tot = ss.tot ? ss.tot[0] : 0.0, acc = ss.acc ? ss.acc[0] : 0.0;
-  int gcur = ss.gcur;
+  int gcur = ss.gcur, gord = 0;
   bool first_group = ss.first_group != 0;
   for (int s = 0; s < nsrc; s++) {
-    const int gs = group_start(nsrc_total, nw, s0 + s);
+    const int gs = gstart[s0 + s];
     if (s0 + s > 0 && gs != gcur) {
-      tot = first_group ? acc : tot + acc;
+      if (per_group) out[gord] = acc;
+      else tot = first_group ? acc : tot + acc;
       first_group = false;
       acc = 0.0;
       gcur = gs;
+      gord++;
     }
     acc += 0.5 * misf[s];
   }
   if (ss.final_chunk) {
-    *out = first_group ? acc : tot + acc;
+    if (per_group) out[gord] = acc;
+    else *out = first_group ? acc : tot + acc;
   } else {
     ss.acc[0] = acc;
     ss.tot[0] = tot;
@@ -975,7 +970,9 @@ __global__ void adj_misfit_kernel(const double* misf, int nsrc, int s0, int nsrc
 }
 
 namespace eik {
-static int host_group_start(int nsrc, int nw, int s) {
+// Source groups (distribsrcs, eikutils.jl:171-190): first source of the group of s when
+// nsrc sources are split into nw groups.
+int host_group_start(int nsrc, int nw, int s) {
   if (nw <= 1) return 0;
   if (nsrc < nw) return s;
   const int dis = nsrc / nw, resto = nsrc % nw;
@@ -988,18 +985,15 @@ static int host_group_start(int nsrc, int nw, int s) {
   return start;
 }
 
-void sum_state_advance(SumState* ss, int nsrc, int s0, int nsrc_total, int nw) {
+void sum_state_advance(SumState* ss, int nsrc, int s0, const int32_t* gstart) {
   for (int s = 0; s < nsrc; s++) {
-    const int gs = host_group_start(nsrc_total, nw, s0 + s);
+    const int gs = gstart[s0 + s];
     if (s0 + s > 0 && gs != ss->gcur) {
       ss->first_group = 0;
       ss->gcur = gs;
     }
   }
 }
-}  // namespace eik
-
-namespace eik {
 
 void gradient_footprint(const Model& m, const eik_extra& ep, long long nrec, int32_t whichgrad,
                         size_t* per_source, size_t* fixed) {
@@ -1019,7 +1013,7 @@ void gradient_footprint(const Model& m, const eik_extra& ep, long long nrec, int
   if (refine) per += nf * (8 + 1 + 1 + 4 + 4 + 1) + sizeof(CoarseProblem) + 8 * (4 + 8) + nf * (8 + 8 + 1) + 1;
   per += N * (8 + 8ull * nd + 8) + 8 + seedcap * 4 * 8 + nd * 8 + (refine ? nf * (8 + 8ull * nd) : 16) +
          sizeof(AdjProblem);
-  per += 3ull * nd * 8 + 8;  // coordinates, receiver offsets, source-location gradient
+  per += 3ull * nd * 8 + 8 + 4;  // coordinates, receiver offsets, source-location gradient, group start
   const bool smoothing = (whichgrad == 1 || whichgrad == 3) && ep.smoothgradkern > 0;
   unsigned long long fix = N * 8 + (smoothing ? N * 8 : 0) + (unsigned long long)std::max<long long>(nrec, 1) *
                                                                  (8ull * nd + 16) + 8192;
@@ -1069,14 +1063,26 @@ int validate_gradient(eik_ctx* ctx, const Model& m, int64_t nsrc, int32_t whichg
 int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
                          const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
                          const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit,
-                         eik_stats* stats, GradTail* tail_out, GradChunk* chunk) {
+                         eik_stats* stats, GradTail* tail_out, GradChunk* chunk, const GroupSpec* groups) {
   int rc = EIK_OK;
   cudaStream_t st = ctx->stream;
   Scratch& S = ctx->scratch;
   const int nd = m.g.nd;
   const long long N = m.N;
-  // :sharedmem splits the sources into groups with separate gradient buffers
+  if (groups && chunk) return fail(ctx, EIK_ERR_ASSERT, "per-group outputs are computed in one pipeline");
+  // :sharedmem splits the sources into groups with separate gradient buffers; explicit
+  // groups (one per request of a merged call) each get their own outputs
   const int ngroups = (ep.parallelkind == 1 && ep.nthreads > 1) ? ep.nthreads : 1;
+  const int nsrc_total = chunk ? chunk->nsrc_total : (int)nsrc;
+  std::vector<int32_t> hgs((size_t)nsrc_total);
+  if (groups) {
+    for (int64_t gi = 0; gi < groups->ngroups; gi++)
+      for (int64_t q = groups->off[gi]; q < groups->off[gi + 1]; q++) hgs[(size_t)q] = (int32_t)groups->off[gi];
+  } else {
+    for (int q = 0; q < nsrc_total; q++) hgs[(size_t)q] = host_group_start(nsrc_total, ngroups, q);
+  }
+  const int per_group = groups ? 1 : 0;
+  const long long nout = groups ? groups->ngroups : 1;  // gradient fields and misfits written
   const bool wantvel = whichgrad == 1 || whichgrad == 3;
   ForwardState fw;
   rc = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
@@ -1106,8 +1112,10 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   const long long nker = smoothing ? (nd == 3 ? (long long)ep.smoothgradkern * ep.smoothgradkern * ep.smoothgradkern
                                               : (long long)ep.smoothgradkern * ep.smoothgradkern)
                                    : 1;
-  GET(gsum, double, "adj_gradsum", smoothing ? N : 1);
+  GET(gsum, double, "adj_gradsum", smoothing ? nout * N : 1);
   GET(gw, double, "adj_smooth_w", nker);
+  int32_t* dgs;
+  GET(dgs, int32_t, "adj_gstart", nsrc_total);
   GET(dap, AdjProblem, "adj_probs", nsrc);
   GET(dfb, ForwardBatch, "adj_fb", 1);
   GET(dwarn, uint32_t, "adj_warn", 1);
@@ -1120,7 +1128,9 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   }
   const void* hap_src = stage_host(ctx, hap.data(), sizeof(AdjProblem) * nsrc);
   const void* fb_src = stage_host(ctx, &fw.fb, sizeof(ForwardBatch));
-  if (!hap_src || !fb_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
+  const void* gs_src = stage_host(ctx, hgs.data(), sizeof(int32_t) * hgs.size());
+  if (!hap_src || !fb_src || !gs_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
+  CUDA_OK(ctx, cudaMemcpyAsync(dgs, gs_src, sizeof(int32_t) * hgs.size(), cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemcpyAsync(dap, hap_src, sizeof(AdjProblem) * nsrc, cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemcpyAsync(dfb, fb_src, sizeof(ForwardBatch), cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemsetAsync(dwarn, 0, sizeof(uint32_t), st));
@@ -1157,9 +1167,9 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   ta.nsrc = (int)nsrc;
   ta.refine = ep.refinearoundsrc;
   ta.whichgrad = whichgrad;
-  ta.ngroups = ngroups;
+  ta.gstart = dgs;
   ta.s0 = chunk ? chunk->s0 : 0;
-  ta.nsrc_total = chunk ? chunk->nsrc_total : (int)nsrc;
+  ta.nsrc_total = nsrc_total;
   ta.prevbuf = (chunk && chunk->prev_valid) ? chunk->prevbuf : nullptr;
   ta.probs = dprobs;
   ta.ap = dap;
@@ -1187,7 +1197,7 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
     ss.gcur = chunk ? chunk->gcur : 0;
     ss.final_chunk = chunk ? (chunk->final_chunk ? 1 : 0) : 1;
     if (d_gradvel)
-      adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ta.s0, ta.nsrc_total, ngroups, N, ss,
+      adj_sum_kernel<<<ctx->nsm * 8, 256, 0, st>>>(dap, (int)nsrc, ta.s0, dgs, per_group, N, ss,
                                                    smoothing ? gsum : d_gradvel);
     if (chunk && !chunk->final_chunk) {
       // the group buffer as this chunk leaves it: its last source's final field
@@ -1200,7 +1210,8 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
       const void* w_src = stage_host(ctx, w.data(), sizeof(double) * w.size());
       if (!w_src) return fail(ctx, EIK_ERR_CUDA, "cudaMallocHost of a plan's staging copy failed");
       CUDA_OK(ctx, cudaMemcpyAsync(gw, w_src, sizeof(double) * w.size(), cudaMemcpyHostToDevice, st));
-      CUDA_OK(ctx, launch_smoothgrad(m.g, (int)ep.smoothgradkern, gw, gsum, d_gradvel, st));
+      for (long long q = 0; q < nout; q++)
+        CUDA_OK(ctx, launch_smoothgrad(m.g, (int)ep.smoothgradkern, gw, gsum + q * N, d_gradvel + q * N, st));
     }
   }
   if (d_misfit) {
@@ -1210,13 +1221,13 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
     ms.first_group = chunk ? chunk->first_group : 1;
     ms.gcur = chunk ? chunk->gcur : 0;
     ms.final_chunk = chunk ? (chunk->final_chunk ? 1 : 0) : 1;
-    adj_misfit_kernel<<<1, 1, 0, st>>>(misf, (int)nsrc, ta.s0, ta.nsrc_total, ngroups, ms, d_misfit);
+    adj_misfit_kernel<<<1, 1, 0, st>>>(misf, (int)nsrc, ta.s0, dgs, per_group, ms, d_misfit);
   }
   if (chunk) {
     SumState adv;
     adv.first_group = chunk->first_group;
     adv.gcur = chunk->gcur;
-    sum_state_advance(&adv, (int)nsrc, chunk->s0, chunk->nsrc_total, ngroups);
+    sum_state_advance(&adv, (int)nsrc, chunk->s0, hgs.data());
     chunk->first_group = adv.first_group;
     chunk->gcur = adv.gcur;
     chunk->prev_valid = true;
@@ -1229,7 +1240,8 @@ int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs
   tail.dwarn = dwarn;
   tail.arounds = aa.sa.rs.rounds;
   tail.launches = 7 + (d_misfit ? 1 : 0) +
-                  (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0) + (smoothing ? 1 : 0);
+                  (wantvel ? 3 + (ep.radiussmoothgradsrc > 0 ? 1 : 0) + (d_gradvel ? 1 : 0) : 0) +
+                  (smoothing ? (int)nout : 0);
   if (tail_out) *tail_out = tail;
   if (ctx->capturing) return EIK_OK;  // read back after each replay of the captured graph
   rc = gradient_tail_stats(ctx, tail, stats);
@@ -1346,6 +1358,7 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
                             double* gradsrc, double* misfit, eik_stats* stats) {
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;
@@ -1420,6 +1433,83 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
   return EIK_OK;
 }
 
+extern "C" int eik_gradient_groups(eik_ctx* ctx, eik_model_id model, int64_t ngroups, const int64_t* group_off,
+                                   const double* coordsrc, const int64_t* rec_off, const double* rec,
+                                   const double* pickobs, const double* stdobs, int32_t whichgrad,
+                                   const eik_extra* ep_in, double* gradvel, double* gradsrc, double* misfit,
+                                   eik_stats* stats) {
+  if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
+  if (ngroups < 1 || !group_off) return fail(ctx, EIK_ERR_ASSERT, "ngroups >= 1 and NULL argument");
+  if (group_off[0] != 0) return fail(ctx, EIK_ERR_ASSERT, "group_off[0] must be 0");
+  for (int64_t gi = 0; gi < ngroups; gi++)
+    if (group_off[gi + 1] <= group_off[gi]) return fail(ctx, EIK_ERR_ASSERT, "every group has at least one source");
+  const int64_t nsrc = group_off[ngroups];
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
+  auto it = ctx->models.find(model);
+  if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
+  const Model& m = it->second;
+  eik_extra ep;
+  if (ep_in) ep = *ep_in;
+  else eik_extra_defaults(&ep);
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  int rc = validate_gradient(ctx, m, nsrc, whichgrad, ep);
+  if (rc) return rc;
+  if (!coordsrc || !rec_off || !rec || !pickobs || !stdobs) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
+  rc = check_positions(ctx, m.g, nsrc, coordsrc, rec_off, rec);
+  if (rc) return rc;
+  const long long N = m.N, nrec = rec_off[nsrc];
+  if (gradient_chunk(ctx, m, ep, nsrc, nrec, whichgrad) < nsrc)
+    return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "a call with per-group outputs runs in one pipeline: it exceeds the HBM "
+                                            "budget");
+  CUDA_OK(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  Scratch& S = ctx->scratch;
+  const int nd = m.g.nd;
+#define GET(var, type, name, count)                                                  \
+  var = (type*)S.get(name, sizeof(type) * (size_t)(count), &rc);                     \
+  if (!var) return rc == EIK_ERR_OUT_OF_BUDGET                                       \
+                     ? fail(ctx, rc, "scratch '%s' exceeds the HBM budget", name)    \
+                     : fail(ctx, rc, "cudaMalloc of scratch '%s' failed", name);
+  double *d_cs, *d_rec, *d_po, *d_so, *d_gv, *d_gs, *d_m;
+  long long* d_off;
+  GET(d_cs, double, "in_cs", nsrc * nd);
+  GET(d_rec, double, "in_rec", std::max<long long>(nrec, 1) * nd);
+  GET(d_po, double, "in_pickobs", std::max<long long>(nrec, 1));
+  GET(d_so, double, "in_stdobs", std::max<long long>(nrec, 1));
+  GET(d_gv, double, "out_gradvel", ngroups * N);
+  GET(d_gs, double, "out_gradsrc", nsrc * nd);
+  GET(d_m, double, "out_misfit", ngroups);
+  GET(d_off, long long, "in_off", nsrc + 1);
+#undef GET
+  cudaEventRecord(ctx->ev0, st);
+  CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
+  CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
+  if (nrec) {
+    CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
+    CUDA_OK(ctx, cudaMemcpyAsync(d_po, pickobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
+    CUDA_OK(ctx, cudaMemcpyAsync(d_so, stdobs, sizeof(double) * nrec, cudaMemcpyHostToDevice, st));
+  }
+  const bool wantvel = whichgrad == 1 || whichgrad == 3, wantsrc = whichgrad != 1;
+  const GroupSpec gsp{ngroups, group_off};
+  rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
+                     wantsrc ? d_gs : nullptr, d_m, stats, nullptr, nullptr, &gsp);
+  if (rc) return rc;
+  if (misfit) CUDA_OK(ctx, cudaMemcpyAsync(misfit, d_m, sizeof(double) * ngroups, cudaMemcpyDeviceToHost, st));
+  if (gradvel && wantvel)
+    CUDA_OK(ctx, cudaMemcpyAsync(gradvel, d_gv, sizeof(double) * ngroups * N, cudaMemcpyDeviceToHost, st));
+  if (gradsrc && wantsrc)
+    CUDA_OK(ctx, cudaMemcpyAsync(gradsrc, d_gs, sizeof(double) * nsrc * nd, cudaMemcpyDeviceToHost, st));
+  cudaEventRecord(ctx->ev1, st);
+  CUDA_OK(ctx, cudaStreamSynchronize(st));
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    stats->device_ms = ms;
+  }
+  return EIK_OK;
+}
+
 extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double* coordsrc_dev,
                                    const int64_t* rec_off, const double* rec_dev, const double* pickobs_dev,
                                    const double* stdobs_dev, int32_t whichgrad, const eik_extra* ep_in,
@@ -1427,6 +1517,7 @@ extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsr
                                    eik_stats* stats) {
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;

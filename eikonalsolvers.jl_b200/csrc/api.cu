@@ -37,22 +37,30 @@ int fail(eik_ctx* ctx, int code, const char* fmt, ...) {
 // -------------------------------------------------------------------- scratch --
 void* Scratch::get(const std::string& name, size_t bytes, int* rc) {
   auto it = bufs.find(name);
-  if (it != bufs.end() && it->second.bytes >= bytes) return it->second.ptr;
+  if (it != bufs.end() && it->second.bytes >= bytes) {
+    it->second.used = epoch;
+    return it->second.ptr;
+  }
   if (it != bufs.end()) {
     cudaFree(it->second.ptr);
     total -= it->second.bytes;
     bufs.erase(it);
   }
+  if (total + bytes > budget) release_unused();
   if (total + bytes > budget) {
     *rc = EIK_ERR_OUT_OF_BUDGET;
     return nullptr;
   }
   void* p = nullptr;
   if (cudaMalloc(&p, std::max<size_t>(bytes, 256)) != cudaSuccess) {
-    *rc = EIK_ERR_CUDA;
-    return nullptr;
+    cudaGetLastError();  // clear the allocation error before trying again
+    release_unused();
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 256)) != cudaSuccess) {
+      *rc = EIK_ERR_CUDA;
+      return nullptr;
+    }
   }
-  bufs[name] = Buf{p, bytes};
+  bufs[name] = Buf{p, bytes, epoch};
   total += bytes;
   return p;
 }
@@ -60,6 +68,17 @@ void Scratch::release_all() {
   for (auto& kv : bufs) cudaFree(kv.second.ptr);
   bufs.clear();
   total = 0;
+}
+void Scratch::release_unused() {
+  for (auto it = bufs.begin(); it != bufs.end();) {
+    if (it->second.used != epoch) {
+      cudaFree(it->second.ptr);  // waits for the device work that may still read it
+      total -= it->second.bytes;
+      it = bufs.erase(it);
+    } else {
+      ++it;
+    }
+  }
 }
 
 // ----------------------------------------------------------------- grids --
@@ -192,6 +211,10 @@ int model_create(eik_ctx* ctx, const eik_grid* grd, const double* vel, bool dev,
   if (rc) return rc;
   m.N = npts(m.g);
   const size_t bytes = sizeof(double) * (size_t)m.N;
+  if (ctx->scratch.total + ctx->model_bytes + 2 * bytes > ctx->scratch.budget) {
+    ctx->scratch.begin_call();  // scratch kept from earlier calls gives way to a resident model
+    ctx->scratch.release_unused();
+  }
   if (ctx->scratch.total + ctx->model_bytes + 2 * bytes > ctx->scratch.budget)
     return fail(ctx, EIK_ERR_OUT_OF_BUDGET, "model of %zu bytes exceeds the HBM budget", 2 * bytes);
   CUDA_OK(ctx, cudaSetDevice(ctx->device));
@@ -649,6 +672,7 @@ int eik_selftest_wait(eik_ctx* ctx, double timeout_s) {
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   if (!(timeout_s >= 1e-3 && timeout_s <= 10.0)) return fail(ctx, EIK_ERR_ASSERT, "timeout_s must be in [0.001, 10]");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   CUDA_OK(ctx, cudaSetDevice(ctx->device));
   int rc = EIK_OK;
   unsigned int* flag = (unsigned int*)ctx->scratch.get("selftest_flag", 2 * sizeof(unsigned int), &rc);
@@ -698,6 +722,7 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
                    double* ttgrids, eik_stats* stats) {
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;
@@ -754,6 +779,7 @@ int eik_traveltime_multi(eik_ctx* ctx, int64_t nmodel, const eik_model_id* model
   if (nmodel < 1 || !model_ids || !src_off) return fail(ctx, EIK_ERR_ASSERT, "nmodel >= 1 and NULL argument");
   if (nmodel > (1 << 20)) return fail(ctx, EIK_ERR_ASSERT, "more than 2^20 models in one call");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   std::vector<const Model*> mods(nmodel);
   for (int64_t i = 0; i < nmodel; i++) {
     auto it = ctx->models.find(model_ids[i]);

@@ -266,6 +266,7 @@ extern "C" int eik_tracerays(eik_ctx* ctx, const eik_grid* grd, int64_t nsrc, co
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   if (!grd || !ttgrids) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   if (stats) std::memset(stats, 0, sizeof *stats);
   GridDesc g;
   int rc = make_griddesc(ctx, grd, &g);
@@ -302,6 +303,7 @@ extern "C" int eik_traveltime_rays(eik_ctx* ctx, eik_model_id model, int64_t nsr
                                    eik_stats* stats) {
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->scratch.begin_call();
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;

@@ -21,16 +21,23 @@
 namespace eik {
 
 // Grow-only named device buffers, bounded by the context's HBM budget.
+// Named device buffers kept from call to call (grown on demand) under an HBM budget. A
+// call that would exceed the budget, or whose cudaMalloc fails, first frees the buffers no
+// part of the current call has taken (begin_call starts a call), then tries once more.
 struct Scratch {
   struct Buf {
     void* ptr;
     size_t bytes;
+    unsigned used;  // epoch of the last call that took it
   };
   std::map<std::string, Buf> bufs;
   size_t total = 0;
   size_t budget = 0;
+  unsigned epoch = 1;
+  void begin_call() { epoch++; }
   void* get(const std::string& name, size_t bytes, int* rc);
   void release_all();
+  void release_unused();
 };
 
 struct Model {
@@ -116,10 +123,19 @@ struct GradChunk {
 // not grow with the sources.
 void gradient_footprint(const Model& m, const eik_extra& ep, long long nrec, int32_t whichgrad,
                         size_t* per_source, size_t* fixed);
+// Explicit source groups of one call (host offsets, ngroups + 1 values from 0 to nsrc):
+// each group has its own gradient buffer, carry-over and outputs (gradient field, misfit),
+// as a call of that group's sources alone.
+struct GroupSpec {
+  int64_t ngroups;
+  const int64_t* off;
+};
+// Source groups of distribsrcs (eikutils.jl:171-190): first source of the group of s.
+int host_group_start(int nsrc, int nw, int s);
 int gradient_core(eik_ctx* ctx, const Model& m, int64_t nsrc, const double* d_cs, const long long* d_off,
                   const double* d_rec, const double* d_po, const double* d_so, int32_t whichgrad,
                   const eik_extra& ep, double* d_gradvel, double* d_gradsrc, double* d_misfit, eik_stats* stats,
-                  GradTail* tail_out, GradChunk* chunk = nullptr);
+                  GradTail* tail_out, GradChunk* chunk = nullptr, const GroupSpec* groups = nullptr);
 
 }  // namespace eik
 

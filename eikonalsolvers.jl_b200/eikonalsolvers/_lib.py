@@ -24,7 +24,8 @@ EXPORTED = ["eik_extra_defaults", "eik_ctx_create", "eik_ctx_destroy", "eik_last
             "eik_model_upload", "eik_model_upload_device", "eik_model_release", "eik_traveltime",
             "eik_gradient", "eik_gradient_device", "eik_ctx_stream", "eik_ttimemisfit_noalloc",
             "eik_ctx_set_param", "eik_plan_gradient", "eik_plan_run", "eik_plan_destroy", "eik_tracerays",
-            "eik_traveltime_rays", "eik_selftest_wait", "eik_gradient_bytes", "eik_traveltime_multi"]
+            "eik_traveltime_rays", "eik_selftest_wait", "eik_gradient_bytes", "eik_traveltime_multi",
+            "eik_gradient_groups"]
 
 # eik_stats.warn_mask bits and the reference's @warn messages they stand for
 WARNINGS = {
@@ -104,6 +105,9 @@ def load():
         L.eik_traveltime_multi.argtypes = [P, C.c_int64, P, P, P, P, P, C.POINTER(eik_extra), P, P,
                                            C.POINTER(eik_stats)]
         L.eik_traveltime_multi.restype = C.c_int
+        L.eik_gradient_groups.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, P, C.c_int32,
+                                          C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
+        L.eik_gradient_groups.restype = C.c_int
         L.eik_gradient.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, C.c_int32,
                                    C.POINTER(eik_extra), P, P, P, C.POINTER(eik_stats)]
         L.eik_gradient_device.argtypes = [P, C.c_int64, C.c_int64, P, P, P, P, P, C.c_int32,

@@ -250,6 +250,59 @@ class Context:
             return gradsrc, float(misf[0])
         return gradvel, gradsrc, float(misf[0])
 
+    def gradient_groups(self, model: int, grd, groups, whichgrad, extraparams=None):
+        """Several independent gradient evaluations on one model in one device pipeline
+        (eik_gradient_groups): ``groups`` is a list of (coordsrc, coordrec, pickobs, stdobs);
+        returns one result per group, each as ``gradient`` returns it for that group alone
+        with one source group (bit-identical values)."""
+        wg = whichgrad.lstrip(":") if isinstance(whichgrad, str) else whichgrad
+        assert wg in WHICHGRAD, "Symbol 'whichgrad' not in (:gradvel, :gradsrcloc, :gradvelandsrcloc)"
+        assert len(groups) > 0, "at least one group"
+        goff, css, recs, pos, sos = [0], [], [], [], []
+        for coordsrc, coordrec, pickobs, stdobs in groups:
+            cs = np.ascontiguousarray(np.atleast_2d(np.asarray(coordsrc, dtype=np.float64)))
+            if isinstance(coordrec, np.ndarray) and coordrec.dtype != object:
+                coordrec = [coordrec]
+            rr = [np.ascontiguousarray(np.atleast_2d(np.asarray(r, dtype=np.float64))) for r in coordrec]
+            assert cs.shape[0] == len(rr) == len(pickobs) == len(stdobs), "one receiver set per source"
+            for r, p, q in zip(rr, pickobs, stdobs):
+                assert r.shape[0] == np.asarray(p).shape[0], "size(coordrec[r],1)==size(pickobs[r],1)"
+                assert np.asarray(q).shape == np.asarray(p).shape, "size(stdobs[r])==size(pickobs[r])"
+            goff.append(goff[-1] + cs.shape[0])
+            css.append(cs)
+            recs.extend(rr)
+            pos.extend(np.asarray(p, dtype=np.float64).ravel() for p in pickobs)
+            sos.extend(np.asarray(q, dtype=np.float64).ravel() for q in stdobs)
+        ng = len(groups)
+        goff = np.asarray(goff, dtype=np.int64)
+        cs = np.ascontiguousarray(np.concatenate(css, axis=0))
+        nsrc = cs.shape[0]
+        recoff = np.zeros(nsrc + 1, dtype=np.int64)
+        for s, r in enumerate(recs):
+            recoff[s + 1] = recoff[s] + r.shape[0]
+        rec = np.ascontiguousarray(np.concatenate(recs, axis=0))
+        po = np.ascontiguousarray(np.concatenate(pos))
+        so = np.ascontiguousarray(np.concatenate(sos))
+        N = int(np.prod(grd.grsize))
+        gv = np.zeros(ng * N, dtype=np.float64) if wg in ("gradvel", "gradvelandsrcloc") else None
+        gs = np.zeros(nsrc * grd.ndim, dtype=np.float64) if wg in ("gradsrcloc", "gradvelandsrcloc") else None
+        misf = np.zeros(ng, dtype=np.float64)
+        ep = _lib.extra_struct(extraparams)
+        st = _lib.eik_stats()
+        rc = self.L.eik_gradient_groups(self.h, C.c_int64(model), C.c_int64(ng), _lib.ptr(goff), _lib.ptr(cs),
+                                        _lib.ptr(recoff), _lib.ptr(rec), _lib.ptr(po), _lib.ptr(so), WHICHGRAD[wg],
+                                        C.byref(ep), _lib.ptr(gv), _lib.ptr(gs), _lib.ptr(misf), C.byref(st))
+        self.last_stats = st
+        _lib.check(rc, self.h)
+        _warn(st)
+        out = []
+        for g in range(ng):
+            gvel = gv[g * N:(g + 1) * N].reshape(grd.grsize, order="F").copy() if gv is not None else None
+            gsrc = gs.reshape(nsrc, grd.ndim)[goff[g]:goff[g + 1]].copy() if gs is not None else None
+            m = float(misf[g])
+            out.append((gvel, m) if wg == "gradvel" else (gsrc, m) if wg == "gradsrcloc" else (gvel, gsrc, m))
+        return out
+
 
 class GradientPlan:
     """A captured eik_gradient pipeline for fixed model, sources, receivers and parameters,

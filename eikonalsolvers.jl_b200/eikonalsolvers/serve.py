@@ -9,24 +9,30 @@ This loop serves such callers from many threads or processes on one GPU:
 * every worker slot owns a libeikcuda context (its own CUDA stream, scratch memory under
   its own HBM budget, a share of the SMs for the persistent solve kernels), so requests
   taken by different slots run on the GPU at the same time;
-* a slot that becomes free takes the oldest waiting request, together with every other
-  waiting traveltime request on the same model and parameters (up to a source cap): they
-  run as one batched call and the picks are split back per request;
+* a slot that becomes free takes the oldest waiting request, together with the waiting
+  requests it can share a call with (up to a source cap): traveltime requests on any models
+  of the same dimension and parameters (one eik_traveltime_multi pipeline, grids of
+  different sizes side by side), or gradient requests on the same model with the same
+  `whichgrad` and parameters (one eik_gradient_groups pipeline, each request a source group
+  with its own buffer and outputs); the results are split back per request;
 * admission by device memory: with a server-wide ``hbm_budget`` every batch's device
   footprint is estimated (``request_bytes``: the per-node-source state of the forward solve,
   and of the adjoint for gradients, times grid nodes and sources, plus the refined windows),
   and a slot that took a batch waits until the batch fits beside the batches in flight; a
   batch that could not fit even alone fails with an error and the server goes on;
 * a request that does not fit a slot's own HBM budget fails alone (EIK_ERR_OUT_OF_BUDGET);
+* load shedding: with ``max_queue`` > 0 a request that arrives while that many wait is
+  refused at once (its future raises ServerOverloaded) instead of queueing without bound;
+  `stats()` counts the refusals;
 * latency (submission to completion) is recorded per request; `stats()` gives p50/p99 and
   source-solves/s;
 * each call runs with the launch parameters the autotuner's table holds for its workload
   class (the library's choice by size otherwise).
 
 Results do not depend on the mix: the forward traveltimes are the unique fixed point of
-the order rule whatever the batch, and gradient requests are never merged (their
-source-point carry-over would couple them), so each result is identical to the same
-request served alone.
+the order rule whatever the batch, and merged gradient requests keep their own source-point
+carry-over and sums (per-group outputs), so each result is identical to the same request
+served alone.
 """
 from __future__ import annotations
 
@@ -42,6 +48,10 @@ import numpy as np
 from .api import Context
 from .structs import ExtraParams
 from .tune import default_tuner
+
+
+class ServerOverloaded(RuntimeError):
+    """The request queue was full when the request arrived (Server(max_queue=...))."""
 
 
 @dataclass
@@ -80,6 +90,14 @@ def request_bytes(grd, nsrc: int, kind: str, extraparams: Optional[ExtraParams] 
     return int(nsrc) * (n * per + fine)
 
 
+def batch_bytes(batch, models) -> int:
+    """Estimated device memory of one merged call: request_bytes at the largest grid of the
+    batch (the per-source arrays of a multi-model call share that stride) for all its sources."""
+    grds = [models[r.model][1] for r in batch]
+    big = max(grds, key=lambda g: int(np.prod(g.grsize)))
+    return request_bytes(big, sum(r.nsrc for r in batch), batch[0].kind, batch[0].extraparams)
+
+
 def _ep_key(ep: Optional[ExtraParams]):
     if ep is None:
         return None
@@ -91,7 +109,8 @@ class Server:
     """Serves `Request`s on one GPU with `slots` concurrent worker contexts."""
 
     def __init__(self, device: int = 0, slots: int = 2, hbm_budget_per_slot: int = 0,
-                 max_batch_sources: int = 64, context_factory=None, tuner=None, hbm_budget: int = 0):
+                 max_batch_sources: int = 64, context_factory=None, tuner=None, hbm_budget: int = 0,
+                 max_queue: int = 0):
         self.slots = max(1, int(slots))
         self.hbm_budget = int(hbm_budget)  # device bytes the batches in flight may take together (0 = no limit)
         self._inflight = 0
@@ -100,6 +119,8 @@ class Server:
         # launch parameters per workload class (autotuner table; results do not depend on them)
         self.tuner = tuner if tuner is not None else default_tuner()
         self.max_batch_sources = int(max_batch_sources)
+        self.max_queue = int(max_queue)  # waiting requests beyond which arrivals are refused (0 = no limit)
+        self._refused = 0
         make = context_factory or (lambda: Context(device, hbm_budget_per_slot))
         self._ctx = []
         for _ in range(self.slots):
@@ -140,12 +161,22 @@ class Server:
         with self._cv:
             if self._closing:
                 raise RuntimeError("server is closed")
+            if self.max_queue > 0 and len(self._queue) >= self.max_queue:
+                self._refused += 1
+                req.future.set_exception(ServerOverloaded(f"{len(self._queue)} requests are waiting"))
+                return req.future
             self._queue.append(req)
             self._cv.notify()
         return req.future
 
+    def _batch_key(self, r: Request):
+        """Requests with equal keys can share one call."""
+        if r.kind == "traveltime":
+            return ("traveltime", self._models[r.model][1].ndim, _ep_key(r.extraparams))
+        return ("gradient", r.model, r.whichgrad, _ep_key(r.extraparams))
+
     def _take(self) -> Optional[List[Request]]:
-        """Oldest request plus the waiting traveltime requests it can be batched with."""
+        """Oldest request plus the waiting requests it can share a call with."""
         with self._cv:
             while not self._queue and not self._closing:
                 self._cv.wait()
@@ -153,24 +184,22 @@ class Server:
                 return None
             head = self._queue.popleft()
             batch = [head]
-            if head.kind == "traveltime":
-                n = head.nsrc
-                key = (head.model, _ep_key(head.extraparams))
-                grd = self._models[head.model][1]
-                keep = deque()
-                while self._queue:
-                    r = self._queue.popleft()
-                    # with a device-memory budget, a merged batch must still fit it: requests
-                    # that fit alone are not refused only because they were batched together
-                    fits = (self.hbm_budget <= 0 or
-                            request_bytes(grd, n + r.nsrc, "traveltime", head.extraparams) <= self.hbm_budget)
-                    if (r.kind == "traveltime" and (r.model, _ep_key(r.extraparams)) == key
-                            and n + r.nsrc <= self.max_batch_sources and fits):
-                        batch.append(r)
-                        n += r.nsrc
-                    else:
-                        keep.append(r)
-                self._queue = keep
+            key = self._batch_key(head)
+            n = head.nsrc
+            keep = deque()
+            while self._queue:
+                r = self._queue.popleft()
+                # with a device-memory budget, a merged batch must still fit it: requests
+                # that fit alone are not refused only because they were batched together
+                ok = self._batch_key(r) == key and n + r.nsrc <= self.max_batch_sources
+                if ok and self.hbm_budget > 0:
+                    ok = batch_bytes(batch + [r], self._models) <= self.hbm_budget
+                if ok:
+                    batch.append(r)
+                    n += r.nsrc
+                else:
+                    keep.append(r)
+            self._queue = keep
             return batch
 
     def _admit(self, need: int) -> bool:
@@ -199,8 +228,7 @@ class Server:
             batch = self._take()
             if batch is None:
                 return
-            grd0 = self._models[batch[0].model][1]
-            need = request_bytes(grd0, sum(r.nsrc for r in batch), batch[0].kind, batch[0].extraparams)
+            need = batch_bytes(batch, self._models)
             if not self._admit(need):
                 err = MemoryError(f"request needs ~{need} bytes of device memory, the server's budget is "
                                   f"{self.hbm_budget}")
@@ -216,28 +244,19 @@ class Server:
             for r in batch:
                 r.t_start = t0
             try:
-                grd = self._models[batch[0].model][1]
-                mid = self._model_id(slot, batch[0].model)
-                nsrc = sum(r.nsrc for r in batch)
-                if not self.tuner.apply_known(ctx, grd, nsrc, batch[0].extraparams):
-                    ctx.set_param("round_gate", 0.0)  # the library's choice by size
-                    ctx.set_param("ctas_per_sm", 0)
-                if batch[0].kind == "traveltime":
-                    cs = np.vstack([np.atleast_2d(r.coordsrc) for r in batch])
-                    recs = [rr for r in batch for rr in r.coordrec]
-                    picks = ctx.traveltime(mid, grd, cs, recs, extraparams=batch[0].extraparams)
-                    k = 0
+                results = [(True, x) for x in self._run(slot, ctx, batch)]
+            except Exception as e:  # the request fails, the server goes on
+                if len(batch) == 1:
+                    results = [(False, e)]
+                else:
+                    # a merged call failed: each request again on its own, so that a failure
+                    # stays with the request that caused it
                     results = []
                     for r in batch:
-                        results.append(picks[k:k + r.nsrc])
-                        k += r.nsrc
-                else:
-                    r = batch[0]
-                    results = [ctx.gradient(mid, grd, r.coordsrc, r.coordrec, r.pickobs, r.stdobs, r.whichgrad,
-                                            extraparams=r.extraparams)]
-                err = None
-            except Exception as e:  # the request fails, the server goes on
-                err = e
+                        try:
+                            results.append((True, self._run(slot, ctx, [r])[0]))
+                        except Exception as e1:
+                            results.append((False, e1))
             self._release(need)
             t1 = time.perf_counter()
             with self._cv:
@@ -245,18 +264,66 @@ class Server:
                 for i, r in enumerate(batch):
                     r.t_done = t1
                     self._done.append(r)
-            for i, r in enumerate(batch):
-                if err is None:
-                    r.future.set_result(results[i])
+            for (ok, x), r in zip(results, batch):
+                if ok:
+                    r.future.set_result(x)
                 else:
-                    r.future.set_exception(err)
+                    r.future.set_exception(x)
+
+    def _run(self, slot: int, ctx, batch: List[Request]) -> list:
+        """One call for the batch; one result per request, in batch order."""
+        head = batch[0]
+        nsrc = sum(r.nsrc for r in batch)
+        grds = [self._models[r.model][1] for r in batch]
+        big = max(grds, key=lambda g: int(np.prod(g.grsize)))
+        if not self.tuner.apply_known(ctx, big, nsrc, head.extraparams):
+            ctx.set_param("round_gate", 0.0)  # the library's choice by size
+            ctx.set_param("ctas_per_sm", 0)
+        if head.kind == "gradient":
+            grd = grds[0]
+            mid = self._model_id(slot, head.model)
+            if len(batch) == 1:
+                return [ctx.gradient(mid, grd, head.coordsrc, head.coordrec, head.pickobs, head.stdobs,
+                                     head.whichgrad, extraparams=head.extraparams)]
+            return ctx.gradient_groups(mid, grd, [(r.coordsrc, r.coordrec, r.pickobs, r.stdobs) for r in batch],
+                                       head.whichgrad, extraparams=head.extraparams)
+        # traveltime: the requests of each model together, models in order of first appearance
+        order = []
+        for r in batch:
+            if r.model not in order:
+                order.append(r.model)
+        if len(order) == 1:
+            mid = self._model_id(slot, head.model)
+            cs = np.vstack([np.atleast_2d(r.coordsrc) for r in batch])
+            recs = [rr for r in batch for rr in r.coordrec]
+            picks = ctx.traveltime(mid, grds[0], cs, recs, extraparams=head.extraparams)
+        else:
+            reqs = []
+            for key in order:
+                rs = [r for r in batch if r.model == key]
+                reqs.append((self._model_id(slot, key), self._models[key][1],
+                             np.vstack([np.atleast_2d(r.coordsrc) for r in rs]), [rr for r in rs for rr in r.coordrec]))
+            per_model = ctx.traveltime_multi(reqs, extraparams=head.extraparams)
+            by_model = dict(zip(order, per_model))
+            picks = []
+            taken = {k: 0 for k in order}
+            for r in batch:
+                k0 = taken[r.model]
+                picks.extend(by_model[r.model][k0:k0 + r.nsrc])
+                taken[r.model] = k0 + r.nsrc
+        results, k = [], 0
+        for r in batch:
+            results.append(picks[k:k + r.nsrc])
+            k += r.nsrc
+        return results
 
     # ------------------------------------------------------------------- stats --
     def stats(self) -> dict:
         with self._cv:
             done = list(self._done)
+            refused = self._refused
         if not done:
-            return {"requests": 0}
+            return {"requests": 0, "refused": refused}
         lat = np.array([r.t_done - r.t_submit for r in done])
         t0 = min(r.t_submit for r in done)
         t1 = max(r.t_done for r in done)
@@ -264,7 +331,7 @@ class Server:
         return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
                 "source_solves_per_s": nsrc / (t1 - t0) if t1 > t0 else None,
-                "requests_per_s": len(done) / (t1 - t0) if t1 > t0 else None}
+                "requests_per_s": len(done) / (t1 - t0) if t1 > t0 else None, "refused": refused}
 
     def close(self):
         with self._cv:

@@ -200,6 +200,21 @@ int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const do
                         const double* stdobs_dev, int32_t whichgrad, const eik_extra* ep,
                         double* gradvel_dev, double* gradsrc_dev, double* misfit_dev, eik_stats* stats);
 
+/* No counterpart in the reference as one call: calcgradsomesrc (eikmaingrad.jl:174-258) for
+ * several independent gradient evaluations on one model in one pipeline (a serving loop
+ * merging requests). Group g is sources group_off[g]..group_off[g+1]-1 (group_off[0] = 0,
+ * every group non-empty) with its own gradient buffer and carry-over, as the reference's one
+ * worker group; its results equal eik_gradient of those sources alone with one group
+ * (:serial), bit for bit. coordsrc, rec_off, rec, pickobs, stdobs run over all sources as in
+ * eik_gradient; ep applies to every group (its parallelkind and nthreads are not used).
+ * gradvel: nullable, ngroups x N (group g's field at g*N); gradsrc: nullable, nsrc x ndim;
+ * misfit: nullable, ngroups values. The call is not split into chunks: one that exceeds the
+ * HBM budget returns EIK_ERR_OUT_OF_BUDGET. */
+int eik_gradient_groups(eik_ctx* ctx, eik_model_id model, int64_t ngroups, const int64_t* group_off,
+                        const double* coordsrc, const int64_t* rec_off, const double* rec, const double* pickobs,
+                        const double* stdobs, int32_t whichgrad, const eik_extra* ep, double* gradvel,
+                        double* gradsrc, double* misfit, eik_stats* stats);
+
 /* Captured gradient plans (no counterpart in the reference; for callers that evaluate
  * eikgradient model after model with the same sources and receivers, as the HMC problem
  * callables of HMCtraveltimes.jl:84-104 do). eik_plan_gradient validates like eik_gradient,

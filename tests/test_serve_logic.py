@@ -7,7 +7,7 @@ import time
 import numpy as np
 import pytest
 
-from eikonalsolvers import Grid2DCart
+from eikonalsolvers import Grid2DCart, Grid3DCart
 from eikonalsolvers.serve import Request, Server
 
 
@@ -40,6 +40,13 @@ class FakeContext:
             self.calls.append(("traveltime", len(cs)))
         return [cs[s][0] + np.arange(len(recs[s]), dtype=float) for s in range(len(cs))]
 
+    def traveltime_multi(self, reqs, extraparams=None):
+        time.sleep(0.01)
+        with self.lock:
+            self.calls.append(("traveltime_multi", tuple(len(cs) for (_, _, cs, _) in reqs)))
+        return [[cs[s][0] + np.arange(len(recs[s]), dtype=float) for s in range(len(cs))]
+                for (_, _, cs, recs) in reqs]
+
     def gradient(self, mid, grd, cs, recs, po, so, which, extraparams=None):
         time.sleep(0.01)
         if np.any(np.isnan(cs)):
@@ -47,6 +54,14 @@ class FakeContext:
         with self.lock:
             self.calls.append(("gradient", len(cs)))
         return np.full(grd.grsize, float(len(cs))), 1.0
+
+    def gradient_groups(self, mid, grd, groups, which, extraparams=None):
+        time.sleep(0.01)
+        if any(np.any(np.isnan(g[0])) for g in groups):
+            raise RuntimeError("bad source")
+        with self.lock:
+            self.calls.append(("gradient_groups", tuple(len(g[0]) for g in groups)))
+        return [(np.full(grd.grsize, float(len(g[0]))), 1.0) for g in groups]
 
 
 @pytest.fixture
@@ -61,39 +76,63 @@ def _req(kind, xs, model="a"):
                    pickobs=[np.zeros(3)] * len(xs), stdobs=[np.ones(3)] * len(xs))
 
 
-def test_traveltime_requests_on_one_model_are_batched_and_split(grd):
+def test_traveltime_requests_are_batched_across_models_and_split(grd):
     FakeContext.calls = []
+    grd3 = Grid3DCart(hgrid=1.0, cooinit=(0.0, 0.0, 0.0), grsize=(4, 4, 4))
     srv = Server(slots=1, max_batch_sources=10, context_factory=FakeContext)
     srv.register_model("a", np.ones(grd.grsize), grd)
-    srv.register_model("b", np.ones(grd.grsize), grd)
+    srv.register_model("b", np.ones((6, 5)), Grid2DCart(hgrid=1.0, cooinit=(0.0, 0.0), grsize=(6, 5)))
+    srv.register_model("c", np.ones(grd3.grsize), grd3)
     blocker = srv.submit(_req("gradient", [9.0]))  # keeps the only slot busy
     futs = [srv.submit(_req("traveltime", [1.0, 2.0])), srv.submit(_req("traveltime", [3.0], model="b")),
-            srv.submit(_req("traveltime", [4.0, 5.0, 6.0]))]
+            srv.submit(_req("traveltime", [4.0, 5.0, 6.0])),
+            srv.submit(Request(model="c", kind="traveltime", coordsrc=np.array([[7.0, 1.0, 1.0]]),
+                               coordrec=[np.zeros((2, 3))]))]
     blocker.result(timeout=10)
     res = [f.result(timeout=10) for f in futs]
     srv.close()
     assert [float(p[0]) for p in res[0]] == [1.0, 2.0]
     assert [float(p[0]) for p in res[2]] == [4.0, 5.0, 6.0]
     assert [float(p[0]) for p in res[1]] == [3.0]
-    # the two requests on model "a" ran as one call of 5 sources, "b" alone
-    assert ("traveltime", 5) in FakeContext.calls and ("traveltime", 1) in FakeContext.calls
+    assert [float(p[0]) for p in res[3]] == [7.0]
+    # the 2D requests ran as one call: model "a" (5 sources) beside model "b"; 3D alone
+    assert ("traveltime_multi", (5, 1)) in FakeContext.calls and ("traveltime", 1) in FakeContext.calls
     st = srv.stats()
-    assert st["requests"] == 4 and st["p99_ms"] >= st["p50_ms"] > 0
+    assert st["requests"] == 5 and st["p99_ms"] >= st["p50_ms"] > 0
 
 
-def test_gradient_requests_are_never_merged_and_failures_stay_local(grd):
+def test_gradient_requests_on_one_model_share_a_call_and_failures_stay_local(grd):
     FakeContext.calls = []
-    srv = Server(slots=2, context_factory=FakeContext)
+    srv = Server(slots=1, context_factory=FakeContext)
     srv.register_model("a", np.ones(grd.grsize), grd)
+    srv.register_model("b", np.ones(grd.grsize), grd)
+    blocker = srv.submit(_req("traveltime", [9.0]))  # keeps the only slot busy
     good = [srv.submit(_req("gradient", [1.0, 2.0])) for _ in range(3)]
+    other = srv.submit(_req("gradient", [1.0], model="b"))
     bad = srv.submit(_req("gradient", [np.nan]))
+    blocker.result(timeout=10)
     for f in good:
         g, m = f.result(timeout=10)
         assert g[0, 0] == 2.0
+    assert other.result(timeout=10)[0][0, 0] == 1.0
     with pytest.raises(RuntimeError, match="bad source"):
         bad.result(timeout=10)
     srv.close()
+    # one merged call failed on the bad request; each request then ran alone
     assert FakeContext.calls.count(("gradient", 2)) == 3
+    assert ("gradient", 1) in FakeContext.calls  # model "b" is never merged with "a"
+
+
+def test_gradient_groups_merge_without_failures(grd):
+    FakeContext.calls = []
+    srv = Server(slots=1, context_factory=FakeContext)
+    srv.register_model("a", np.ones(grd.grsize), grd)
+    blocker = srv.submit(_req("traveltime", [9.0]))
+    futs = [srv.submit(_req("gradient", [1.0] * (k + 1))) for k in range(3)]
+    blocker.result(timeout=10)
+    assert [f.result(timeout=10)[0][0, 0] for f in futs] == [1.0, 2.0, 3.0]
+    srv.close()
+    assert ("gradient_groups", (1, 2, 3)) in FakeContext.calls
 
 
 def test_slots_get_an_sm_share_and_unknown_models_are_refused(grd):
@@ -155,3 +194,23 @@ def test_traveltime_batches_are_capped_by_the_memory_budget(grd):
         assert srv.max_inflight_seen <= srv.hbm_budget
     finally:
         srv.close()
+
+
+def test_a_full_queue_refuses_arrivals(grd):
+    from eikonalsolvers.serve import ServerOverloaded
+    FakeContext.calls = []
+    srv = Server(slots=1, context_factory=FakeContext, max_queue=2)
+    srv.register_model("a", np.ones(grd.grsize), grd)
+    blocker = srv.submit(_req("gradient", [9.0]))
+    t0 = time.perf_counter()
+    while srv._queue and time.perf_counter() - t0 < 5.0:  # until the slot has taken it
+        time.sleep(0.0005)
+    queued = [srv.submit(_req("traveltime", [1.0])), srv.submit(_req("traveltime", [2.0]))]
+    refused = srv.submit(_req("traveltime", [3.0]))
+    with pytest.raises(ServerOverloaded):
+        refused.result(timeout=10)
+    blocker.result(timeout=10)
+    assert [float(f.result(timeout=10)[0][0]) for f in queued] == [1.0, 2.0]
+    st = srv.stats()
+    srv.close()
+    assert st["refused"] == 1 and st["requests"] == 3
