@@ -475,7 +475,8 @@ def main_b200(args):
     roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind,
             "traffic": (traffic_ss * N * nsrc if traffic_ss is not None else None),
-            "traffic_note": "DRAM bytes per launch scaled from the per-node-solve figure of profiles/<kernel>.md",
+            "traffic_note": "DRAM bytes per launch: the per-node-solve figure of profiles/<kernel>.md (ncu, "
+                            "256^3 x 1 source, same launch parameters) times the node-solves of this launch",
             "algorithmic_bytes_per_launch": alg_bytes, "avg_launch_ms": per_launch_ms,
             "share_of_step": kms / ms,
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in kern.items()}}

@@ -263,6 +263,12 @@ __global__ void adj_rounds_init_kernel(SolveArgs a) {
   *a.abort_flag = 0;
 }
 
+// The node's solve is a chain of dependent L2 round trips; its loads go out in batches: the
+// codes of the node and of the 4*ND nodes that may read it (with the right-hand side), then
+// per axis the coefficient and λ of the dependants on that axis. The terms are subtracted
+// in the same fixed order as they would be one by one (axis, then offset -2, -1, +1, +2).
+// Everything read here was written before this node was listed (the forward's codes and
+// coefficients, and the dependants' λ, each released only after its store and a fence).
 template <int ND>
 __device__ void adj_node(const AdjArgs& aa, int prob, long long l, unsigned long long gb, unsigned int* rel) {
   const SolveArgs& a = aa.sa;
@@ -271,33 +277,68 @@ __device__ void adj_node(const AdjArgs& aa, int prob, long long l, unsigned long
   const GridDesc& g = P.g;
   const long long N = npts(g);
   const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
-  const uint8_t cb = P.code[l];
-  int8_t cm[3];
-  unpack_codes(cb, cm);
-  if ((cb & CODE_SRC_BIT) && P.kL[l] == -EIK_INF) return;  // source points: no unknown
-  double sum = A.rhs[l];
-  double dh[3];
+  long long nl[ND][4];
+  uint8_t ncode[ND][4];
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
-    for (int dl = -2; dl <= 2; dl++) {
-      if (dl == 0) continue;
+    for (int j = 0; j < 4; j++) {
+      const int dl = j < 2 ? j - 2 : j - 1;
+      nl[ax][j] = -1;
+      if (c[ax] + dl < 0 || c[ax] + dl >= g.n[ax]) continue;
       int pr[3] = {c[0], c[1], c[2]};
       pr[ax] += dl;
-      if (pr[ax] < 0 || pr[ax] >= g.n[ax]) continue;
-      const long long lr = lin3(g, pr[0], pr[1], pr[2]);
+      nl[ax][j] = lin3(g, pr[0], pr[1], pr[2]);
+    }
+  const uint8_t cb = P.code[l];
+  const double rhs = A.rhs[l];
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) ncode[ax][j] = nl[ax][j] >= 0 ? P.code[nl[ax][j]] : (uint8_t)CODE_NONE;
+  int8_t cm[3];
+  unpack_codes(cb, cm);
+  if ((cb & CODE_SRC_BIT) && P.kL[l] == -EIK_INF) return;  // source points: no unknown
+  double sum = rhs;
+  double dh[3];
+  double gself[ND];
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++) gself[ax] = A.gdt[(long long)ax * N + l];
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++) {
+    double gv[4], lv[4];
+    int pp[4], acc4[4], sg4[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int dl = j < 2 ? j - 2 : j - 1;
+      pp[j] = 0;
+      if (nl[ax][j] < 0) continue;
       int8_t cd[3];
-      unpack_codes(P.code[lr], cd);
+      unpack_codes(ncode[ax][j], cd);
       const int cc = cd[ax];
       if (cc == 0) continue;
       const int ac = cc < 0 ? -cc : cc;
       const int sg = cc > 0 ? -1 : 1;
       const int p = -dl * sg;
       if (p < 1 || p > ac) continue;
-      node_dh(g, pr[0], dh);
-      const double J = A.gdt[(long long)ax * N + lr] * ((double)sg * dcoeff(ac, p, dh[ax]));
-      sum -= J * __ldcg(A.lam + lr);
+      pp[j] = p;
+      acc4[j] = ac;
+      sg4[j] = sg;
     }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      gv[j] = pp[j] ? A.gdt[(long long)ax * N + nl[ax][j]] : 0.0;
+      lv[j] = pp[j] ? __ldcg(A.lam + nl[ax][j]) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (!pp[j]) continue;
+      const int dl = j < 2 ? j - 2 : j - 1;
+      node_dh(g, c[0] + (ax == 0 ? dl : 0), dh);
+      const double J = gv[j] * ((double)sg4[j] * dcoeff(acc4[j], pp[j], dh[ax]));
+      sum -= J * lv[j];
+    }
+  }
   node_dh(g, c[0], dh);
   double dg = 0.0;
   bool first = true;
@@ -306,7 +347,7 @@ __device__ void adj_node(const AdjArgs& aa, int prob, long long l, unsigned long
     if (cm[ax] == 0) continue;
     const int ac = cm[ax] < 0 ? -cm[ax] : cm[ax];
     const int sg = cm[ax] > 0 ? -1 : 1;
-    const double v = A.gdt[(long long)ax * N + l] * ((double)sg * dcoeff(ac, 0, dh[ax]));
+    const double v = gself[ax] * ((double)sg * dcoeff(ac, 0, dh[ax]));
     dg = first ? v : dg + v;
     first = false;
   }
