@@ -394,11 +394,12 @@ __device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, uns
 // evaluation sees more final neighbours); false evaluates each lane's entry in place. The
 // queue pays on large rounds; on small ones a warp left holding queued entries at the end
 // of a round keeps the others waiting at the barrier.
-#ifndef EIK_FWD_MINBLOCKS
-#define EIK_FWD_MINBLOCKS 4  // CTAs per SM the register budget is sized for
-#endif
-template <int ND, bool QUEUE>
-__global__ void __launch_bounds__(SOLVE_THREADS, EIK_FWD_MINBLOCKS) coarse_rounds_kernel(SolveArgs a) {
+//
+// MB is the number of resident CTAs per SM the register budget is sized for (4: 64
+// registers a thread, 3: 80, 2: 128); the launch's ctas_per_sm selects it. Fewer resident
+// warps with fewer spills pay on large launches, where every SM has work each round.
+template <int ND, bool QUEUE, int MB>
+__global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveArgs a) {
   const int lane = threadIdx.x & 31;
   __shared__ unsigned long long wq[SOLVE_THREADS / 32][QUEUE ? 64 : 1];  // per-warp queue of entries to evaluate
   const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
@@ -746,18 +747,26 @@ void launch_rounds_seed(const SolveArgs& sa, const int32_t* seed_lin, const doub
   else seed_kernel<2><<<sa.nprob, 128, 0, st>>>(sa, seed_lin, seed_tt, out, fine_corners ? 1 : 0, seedcap);
 }
 
-template <int ND, bool QUEUE>
-static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
+template <int ND, bool QUEUE, int MB>
+static cudaError_t launch_solve_mb(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
   const size_t sm = 0;
   int per = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND, QUEUE>, SOLVE_THREADS, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, coarse_rounds_kernel<ND, QUEUE, MB>, SOLVE_THREADS, sm);
   if (ctas_per_sm > 0 && ctas_per_sm < per) per = ctas_per_sm;
   per = per < 1 ? 1 : per;
   SolveArgs args = sa;
   void* kargs[] = {&args};
   // cooperative: every CTA is resident, so the grid barrier between rounds cannot deadlock
-  return cudaLaunchCooperativeKernel((const void*)coarse_rounds_kernel<ND, QUEUE>, dim3(nsm * per),
+  return cudaLaunchCooperativeKernel((const void*)coarse_rounds_kernel<ND, QUEUE, MB>, dim3(nsm * per),
                                      dim3(SOLVE_THREADS), kargs, sm, st);
+}
+
+template <int ND, bool QUEUE>
+static cudaError_t launch_solve_nd(const SolveArgs& sa, int nsm, int ctas_per_sm, cudaStream_t st) {
+  // 2 and 3 resident CTAs per SM take the register budget of that residency; else 4
+  if (ctas_per_sm == 2) return launch_solve_mb<ND, QUEUE, 2>(sa, nsm, ctas_per_sm, st);
+  if (ctas_per_sm == 3) return launch_solve_mb<ND, QUEUE, 3>(sa, nsm, ctas_per_sm, st);
+  return launch_solve_mb<ND, QUEUE, 4>(sa, nsm, ctas_per_sm, st);
 }
 
 cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, int queue, cudaStream_t st) {
