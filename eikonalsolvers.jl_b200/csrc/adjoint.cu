@@ -1400,6 +1400,7 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_gradient");
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;
@@ -1487,6 +1488,7 @@ extern "C" int eik_gradient_groups(eik_ctx* ctx, eik_model_id model, int64_t ngr
   const int64_t nsrc = group_off[ngroups];
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_gradient_groups");
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;
@@ -1559,6 +1561,7 @@ extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsr
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_gradient_device");
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;

@@ -723,6 +723,7 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_traveltime");
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;
@@ -780,6 +781,7 @@ int eik_traveltime_multi(eik_ctx* ctx, int64_t nmodel, const eik_model_id* model
   if (nmodel > (1 << 20)) return fail(ctx, EIK_ERR_ASSERT, "more than 2^20 models in one call");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_traveltime_multi");
   std::vector<const Model*> mods(nmodel);
   for (int64_t i = 0; i < nmodel; i++) {
     auto it = ctx->models.find(model_ids[i]);

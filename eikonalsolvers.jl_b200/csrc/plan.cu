@@ -204,6 +204,7 @@ extern "C" int eik_plan_run(eik_plan* p, const double* vel, const double* pickob
   eik_ctx* ctx = p->ctx;
   if (p->nrec && (!pickobs || !stdobs)) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
   std::lock_guard<std::mutex> lk(ctx->mu);
+  NvtxRange nvtx_call("eik_plan_run");
   auto it = ctx->models.find(p->model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "the plan's model is gone");
   Model& m = it->second;

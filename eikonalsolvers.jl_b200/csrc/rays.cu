@@ -267,6 +267,7 @@ extern "C" int eik_tracerays(eik_ctx* ctx, const eik_grid* grd, int64_t nsrc, co
   if (!grd || !ttgrids) return fail(ctx, EIK_ERR_ASSERT, "NULL argument");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_tracerays");
   if (stats) std::memset(stats, 0, sizeof *stats);
   GridDesc g;
   int rc = make_griddesc(ctx, grd, &g);
@@ -304,6 +305,7 @@ extern "C" int eik_traveltime_rays(eik_ctx* ctx, eik_model_id model, int64_t nsr
   if (!ctx) return fail(ctx, EIK_ERR_ASSERT, "NULL context");
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->scratch.begin_call();
+  NvtxRange nvtx_call("eik_traveltime_rays");
   auto it = ctx->models.find(model);
   if (it == ctx->models.end()) return fail(ctx, EIK_ERR_ASSERT, "unknown model id %lld", (long long)model);
   const Model& m = it->second;

@@ -10,6 +10,7 @@
 
 #include "../../include/eikcuda.h"
 #include "kernels.cuh"
+#include <nvtx3/nvToolsExt.h>
 
 #define CUDA_OK(ctx, call)                                                                      \
   do {                                                                                          \
@@ -24,6 +25,15 @@ namespace eik {
 // Named device buffers kept from call to call (grown on demand) under an HBM budget. A
 // call that would exceed the budget, or whose cudaMalloc fails, first frees the buffers no
 // part of the current call has taken (begin_call starts a call), then tries once more.
+// A named NVTX range over a scope (header-only NVTX 3: a no-op unless a profiler is
+// attached). Entry points open one for their whole call, which ends after the device work.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 struct Scratch {
   struct Buf {
     void* ptr;

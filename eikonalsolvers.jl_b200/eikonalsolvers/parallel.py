@@ -11,12 +11,22 @@ gradient with `world` threads.
 
 The only exchange is one all-reduce of the summed gradient (N values) and the misfit, and
 an all-gather of picks / source gradients: the path has no other communication.
+
+Failure detection: before any result is exchanged every rank reports whether its shard
+succeeded (one all-gather of a status word, the same collective steps on every rank); when a
+shard failed, every rank raises ShardFailed naming the failed ranks, instead of waiting for a
+result that will not come. A rank that dies outright is detected by the process group's
+timeout (or the backend's broken connection) at that first exchange.
 """
 from __future__ import annotations
 
 from typing import Callable, List, Optional, Tuple
 
 import numpy as np
+
+
+class ShardFailed(RuntimeError):
+    """A rank's shard of the sources failed; raised on every rank."""
 
 
 def distribsrcs(nsrc: int, nw: int) -> List[Tuple[int, int]]:
@@ -62,19 +72,30 @@ def eikgradient_sharded(vel, grd, coordsrc, coordrec, pickobs, stdobs, whichgrad
     gv = np.zeros(N, dtype=np.float64)
     gs = np.zeros((nsrc, nd), dtype=np.float64)
     misf = 0.0
+    err = None
     if rng is not None:
         s0, s1 = rng
-        res = local(vel, grd, np.asarray(coordsrc)[s0:s1], coordrec[s0:s1], pickobs[s0:s1], stdobs[s0:s1], wg,
-                    extraparams)
-        if wg == "gradvel":
-            gv = np.asarray(res[0], dtype=np.float64).ravel(order="F")
-        elif wg == "gradsrcloc":
-            gs[s0:s1] = res[0]
-        else:
-            gv = np.asarray(res[0], dtype=np.float64).ravel(order="F")
-            gs[s0:s1] = res[1]
-        misf = float(res[-1])
+        try:
+            res = local(vel, grd, np.asarray(coordsrc)[s0:s1], coordrec[s0:s1], pickobs[s0:s1], stdobs[s0:s1], wg,
+                        extraparams)
+            if wg == "gradvel":
+                gv = np.asarray(res[0], dtype=np.float64).ravel(order="F")
+            elif wg == "gradsrcloc":
+                gs[s0:s1] = res[0]
+            else:
+                gv = np.asarray(res[0], dtype=np.float64).ravel(order="F")
+                gs[s0:s1] = res[1]
+            misf = float(res[-1])
+        except Exception as e:  # reported to every rank below
+            err = e
     dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else "cpu"
+    status = [torch.zeros(1, dtype=torch.float64, device=dev) for _ in range(world)]
+    dist.all_gather(status, torch.tensor([1.0 if err is not None else 0.0], dtype=torch.float64, device=dev),
+                    group=group)
+    failed = [r for r, f in enumerate(status) if float(f.item()) != 0.0]
+    if failed:
+        raise ShardFailed(f"the source shard of rank(s) {failed} failed" + (f": {err}" if err is not None else "")) \
+            from err
     # group sums in group order: g0 + g1 + ... (a sum of two terms is order independent)
     parts = [torch.zeros(N + 1, dtype=torch.float64, device=dev) for _ in range(world)]
     mine = torch.from_numpy(np.concatenate([gv, [misf]])).to(dev)

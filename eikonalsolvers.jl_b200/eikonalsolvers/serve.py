@@ -21,6 +21,8 @@ This loop serves such callers from many threads or processes on one GPU:
   and a slot that took a batch waits until the batch fits beside the batches in flight; a
   batch that could not fit even alone fails with an error and the server goes on;
 * a request that does not fit a slot's own HBM budget fails alone (EIK_ERR_OUT_OF_BUDGET);
+* cancellation: a request whose future was cancelled (``Future.cancel()``) before a slot
+  took it is dropped from the queue and never reaches the GPU;
 * load shedding: with ``max_queue`` > 0 a request that arrives while that many wait is
   refused at once (its future raises ServerOverloaded) instead of queueing without bound;
   `stats()` counts the refusals;
@@ -121,6 +123,7 @@ class Server:
         self.max_batch_sources = int(max_batch_sources)
         self.max_queue = int(max_queue)  # waiting requests beyond which arrivals are refused (0 = no limit)
         self._refused = 0
+        self._cancelled = 0
         make = context_factory or (lambda: Context(device, hbm_budget_per_slot))
         self._ctx = []
         for _ in range(self.slots):
@@ -178,11 +181,15 @@ class Server:
     def _take(self) -> Optional[List[Request]]:
         """Oldest request plus the waiting requests it can share a call with."""
         with self._cv:
-            while not self._queue and not self._closing:
-                self._cv.wait()
-            if not self._queue:
-                return None
-            head = self._queue.popleft()
+            while True:
+                while not self._queue and not self._closing:
+                    self._cv.wait()
+                if not self._queue:
+                    return None
+                head = self._queue.popleft()
+                if head.future.set_running_or_notify_cancel():
+                    break
+                self._cancelled += 1  # cancelled while waiting: dropped
             batch = [head]
             key = self._batch_key(head)
             n = head.nsrc
@@ -194,7 +201,9 @@ class Server:
                 ok = self._batch_key(r) == key and n + r.nsrc <= self.max_batch_sources
                 if ok and self.hbm_budget > 0:
                     ok = batch_bytes(batch + [r], self._models) <= self.hbm_budget
-                if ok:
+                if r.future.cancelled():
+                    self._cancelled += 1
+                elif ok and r.future.set_running_or_notify_cancel():
                     batch.append(r)
                     n += r.nsrc
                 else:
@@ -322,8 +331,9 @@ class Server:
         with self._cv:
             done = list(self._done)
             refused = self._refused
+            cancelled = self._cancelled
         if not done:
-            return {"requests": 0, "refused": refused}
+            return {"requests": 0, "refused": refused, "cancelled": cancelled}
         lat = np.array([r.t_done - r.t_submit for r in done])
         t0 = min(r.t_submit for r in done)
         t1 = max(r.t_done for r in done)
@@ -331,7 +341,8 @@ class Server:
         return {"requests": len(done), "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
                 "source_solves_per_s": nsrc / (t1 - t0) if t1 > t0 else None,
-                "requests_per_s": len(done) / (t1 - t0) if t1 > t0 else None, "refused": refused}
+                "requests_per_s": len(done) / (t1 - t0) if t1 > t0 else None, "refused": refused,
+                "cancelled": cancelled}
 
     def close(self):
         with self._cv:

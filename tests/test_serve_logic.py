@@ -214,3 +214,23 @@ def test_a_full_queue_refuses_arrivals(grd):
     st = srv.stats()
     srv.close()
     assert st["refused"] == 1 and st["requests"] == 3
+
+
+def test_cancelled_requests_never_run(grd):
+    FakeContext.calls = []
+    srv = Server(slots=1, context_factory=FakeContext)
+    srv.register_model("a", np.ones(grd.grsize), grd)
+    blocker = srv.submit(_req("gradient", [9.0]))
+    t0 = time.perf_counter()
+    while srv._queue and time.perf_counter() - t0 < 5.0:  # until the slot has taken it
+        time.sleep(0.0005)
+    keep = srv.submit(_req("traveltime", [1.0]))
+    drop = [srv.submit(_req("traveltime", [2.0])), srv.submit(_req("gradient", [3.0]))]
+    assert all(f.cancel() for f in drop)
+    blocker.result(timeout=10)
+    assert float(keep.result(timeout=10)[0][0]) == 1.0
+    st = srv.stats()
+    srv.close()
+    assert st["cancelled"] == 2 and st["requests"] == 2
+    assert ("gradient", 1) in FakeContext.calls and ("traveltime", 1) in FakeContext.calls
+    assert len(FakeContext.calls) == 2  # the blocker and the kept request only
