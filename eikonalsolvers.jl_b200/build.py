@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libeikcuda.so")
-SOURCES = ["api.cu", "fine.cu", "coarse.cu", "adjoint.cu", "noalloc.cu", "smooth.cu", "plan.cu", "rays.cu"]
-HEADERS = ["common.cuh", "stencil.cuh", "kernels.cuh", "runtime.hpp", "rounds.cuh", "rays.cuh"]
+SOURCES = ["api.cu", "fine.cu", "coarse.cu", "cluster.cu", "adjoint.cu", "noalloc.cu", "smooth.cu", "plan.cu", "rays.cu"]
+HEADERS = ["common.cuh", "stencil.cuh", "kernels.cuh", "runtime.hpp", "rounds.cuh", "rays.cuh", "node.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false",
          "-std=c++17", "-Xcompiler", "-fPIC", "--cudart=static", "-Xptxas", "-v"]

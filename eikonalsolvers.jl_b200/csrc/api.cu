@@ -452,10 +452,18 @@ int forward_multi(eik_ctx* ctx, int nmod, const Model* const* models, const int6
     fsa.rs.stride = (unsigned long long)fb.nfmax;
     fsa.activations = sa.activations + 6;  // own counters: the coarse solve's stay separate
     fsa.node_evals = sa.activations + 7;
-    launch_rounds_init(fsa, st);
-    launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
-    CUDA_OK(ctx, launch_coarse_solve(fsa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
-    nlaunch += 3;
+    // the windows are small: one thread-block cluster each when the GPU has room for it
+    bool in_cluster = false;
+    if (ctx->cluster_solve)
+      CUDA_OK(ctx, launch_cluster_solve(fsa, fb.nfmax, fseed_lin, fseed_tt, fb.out, true, 8, st, &in_cluster));
+    if (in_cluster) {
+      nlaunch += 2;
+    } else {
+      launch_rounds_init(fsa, st);
+      launch_rounds_seed(fsa, fseed_lin, fseed_tt, fb.out, true, 8, st);
+      CUDA_OK(ctx, launch_coarse_solve(fsa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
+      nlaunch += 3;
+    }
     for (int i = 0; i < nmod; i++) {
       const int64_t o = src_off[i];
       if (src_off[i + 1] == o) continue;
@@ -475,13 +483,24 @@ int forward_multi(eik_ctx* ctx, int nmod, const Model* const* models, const int6
   }
   if (!ctx->capturing) cudaEventRecord(ctx->evk[1], st);
   CUDA_OK(ctx, cudaGetLastError());
-  launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
-  CUDA_OK(ctx, cudaGetLastError());
-  if (!ctx->capturing) cudaEventRecord(ctx->evk[2], st);
-  CUDA_OK(ctx, launch_coarse_solve(sa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
-  if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
-  CUDA_OK(ctx, cudaGetLastError());
-  nlaunch += 4;  // coarse init, round init, seeds, solve
+  if (ctx->cluster_solve && cluster_solve_fits(sa, N)) {
+    // small grids: one thread-block cluster per source, init and seeds included
+    if (!ctx->capturing) cudaEventRecord(ctx->evk[2], st);
+    bool in_cluster = false;
+    CUDA_OK(ctx, launch_cluster_solve(sa, N, fb.seed_lin, fb.seed_tt, fb.out, false, fb.seedcap, st, &in_cluster));
+    if (!in_cluster) return fail(ctx, EIK_ERR_CUDA, "the cluster solve could not be launched");
+    if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
+    CUDA_OK(ctx, cudaGetLastError());
+    nlaunch += 2;  // counters, solve
+  } else {
+    launch_coarse_init(hp.data(), dp, (int)nsrc, fb, sa, st);
+    CUDA_OK(ctx, cudaGetLastError());
+    if (!ctx->capturing) cudaEventRecord(ctx->evk[2], st);
+    CUDA_OK(ctx, launch_coarse_solve(sa, sms, ctx->ctas_per_sm, ctx->fwd_queue, st));
+    if (!ctx->capturing) cudaEventRecord(ctx->evk[3], st);
+    CUDA_OK(ctx, cudaGetLastError());
+    nlaunch += 4;  // coarse init, round init, seeds, solve
+  }
   fw->fb = fb;
   fw->sa = sa;
   fw->t = t;
@@ -633,6 +652,11 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
     if (!(value == -1.0 || value == 0.0 || value == 1.0))
       return fail(ctx, EIK_ERR_ASSERT, "fwd_queue must be -1 (automatic), 0 or 1");
     ctx->fwd_queue = (int)value;
+    return EIK_OK;
+  }
+  if (std::strcmp(name, "cluster_solve") == 0) {
+    if (!(value == 0.0 || value == 1.0)) return fail(ctx, EIK_ERR_ASSERT, "cluster_solve must be 0 or 1");
+    ctx->cluster_solve = (int)value;
     return EIK_OK;
   }
   if (std::strcmp(name, "max_rounds") == 0) {

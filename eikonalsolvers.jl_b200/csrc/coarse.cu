@@ -12,6 +12,7 @@
 // traveltime order. Every wait is bounded (global timer), the number of rounds is bounded;
 // both report through an error word instead of trapping.
 #include "kernels.cuh"
+#include "node.cuh"
 #include "rounds.cuh"
 
 namespace eik {
@@ -118,30 +119,10 @@ extern "C" int eik_phase_read(unsigned long long* out) {
 }
 #define PH_T(v) const long long v = clock64()
 #define PH_ADD(k, t0) if ((threadIdx.x & 31) == 0) atomicAdd(&eik_phase[k], (unsigned long long)(clock64() - (t0)))
-#define PL_T(v) const long long v = clock64()
-#define PL_ADD(k, t0) vk[k] += (unsigned long long)(clock64() - (t0))
 #else
 #define PH_T(v)
 #define PH_ADD(k, t0)
-#define PL_T(v)
-#define PL_ADD(k, t0)
 #endif
-// ------------------------------------------------------------------ node solve --
-// Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise.
-__device__ __forceinline__ void node_key(const CoarseProblem& P, long long l, double t, uint8_t cb, double* L, int* d) {
-  if (cb & CODE_SRC_BIT) {
-    *L = __ldcg(P.kL + l);
-    *d = __ldcg(P.kd + l);
-  } else {
-    *L = t;
-    *d = 0;
-  }
-}
-
-// Neighbour directions of a node: k = 4*axis + {0: -2, 1: -1, 2: +1, 3: +2}; bit 12 = itself.
-constexpr int DIR_SELF = 12;
-__device__ __forceinline__ int dir_off(int k) { return (k & 3) < 2 ? (k & 3) - 2 : (k & 3) - 1; }
-
 __device__ __forceinline__ double warp_min(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -152,232 +133,6 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long* p, double v) 
   // traveltimes and potentials are >= 0: their bit patterns order as the values
   if (v < EIK_INF && v < __longlong_as_double((long long)ld_volatile(p)))
     atomicMin(p, (unsigned long long)__double_as_longlong(v));
-}
-
-// One listed node: gate, evaluate, write back. Returns the directions of the nodes to list
-// for the next round (bit DIR_SELF: this node again) and, in *front, the traveltime that
-// bounds their next evaluation from below.
-//
-// The visit is a chain of dependent L2 round trips, which sets the length of a round when
-// fronts are small. Each stage therefore issues all of its loads before it uses any: the
-// node's own state, its immediate neighbours, their codes with the distance-2 nodes, and
-// the relist filter's reads per axis. Reordering these reads does not change what they
-// can observe (see the notes at each stage).
-template <int ND>
-__device__ unsigned process_node(const SolveArgs& a, const CoarseProblem& P, unsigned long long gbase, long long l,
-                                 double T, int r, double* front, unsigned long long* evals,
-                                 unsigned long long* vk) {
-  PL_T(tq0);
-  const GridDesc& g = P.g;
-  const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
-  // The node's own state in one batch. Only this visit writes its t, code and key during
-  // the round (a node is listed once per round), so their order of reading is free.
-  const uint8_t dirty0 = __ldcg(a.rs.dirty + gbase + l);
-  const double tv = __ldcg(a.rs.tent + gbase + l);
-  const uint8_t cb = __ldcg(P.code + l);
-  const double told = __ldcg(P.t + l);
-  // last evaluated value, still valid while nothing the node reads has changed
-  if (!dirty0 && tv > T && tv < EIK_INF) {
-    *front = tv;
-    vk[0]++;
-    return 1u << DIR_SELF;
-  }
-  double Lold;
-  int dold;
-  node_key(P, l, told, cb, &Lold, &dold);
-  if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) {  // source points are fixed
-    vk[1]++;
-    return 0;
-  }
-  // from here the node reads its neighbours' current values: a change after this point
-  // marks it dirty again (writers store the value, fence, then the flag)
-  a.rs.dirty[gbase + l] = 0;
-  __threadfence();
-  // immediate neighbours (one batch with the slowness): potential = smallest traveltime
-  double t1[ND][2];
-  long long l1[ND][2];
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      const int sh = s == 0 ? 1 : -1;
-      l1[ax][s] = -1;
-      if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += sh;
-      l1[ax][s] = lin3(g, p[0], p[1], p[2]);
-    }
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int s = 0; s < 2; s++) t1[ax][s] = l1[ax][s] >= 0 ? __ldcg(P.t + l1[ax][s]) : EIK_INF;
-  const double slow = __ldg(P.slow + l);
-  double pot = EIK_INF;
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int s = 0; s < 2; s++) pot = fmin(pot, t1[ax][s]);
-  if (!(pot < EIK_INF)) {  // nothing reached around it yet
-    a.rs.tent[gbase + l] = EIK_INF;
-    vk[2]++;
-    return 0;
-  }
-  PL_ADD(7, tq0);
-  PL_T(tq1);
-  Nbhd nb;
-  nb_clear(nb);
-  node_dh(g, c[0], nb.dh);
-  nb.slow = slow;
-  nb.c1u = P.c1u;
-  nb.c2u = P.c2u;
-  // Lower bound of the node's value: every term of the local update is at least pot and
-  // the quadratic adds at least (2/3) h s / sqrt(ND) (2nd-order coefficients 9/(4h^2)).
-  // Until the round threshold reaches it the node cannot be final: no evaluation yet.
-  double hmin = nb.dh[0];
-#pragma unroll
-  for (int ax = 1; ax < ND; ax++) hmin = fmin(hmin, nb.dh[ax]);
-  const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * nb.slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
-  if (lb > T) {
-    a.rs.tent[gbase + l] = lb;  // stands, like an evaluated value, while the node stays clean
-    *front = lb;
-    vk[3]++;
-    return 1u << DIR_SELF;
-  }
-  // Codes of the immediate neighbours and the distance-2 nodes with their codes, one batch.
-  // A neighbour's key is read after its traveltime here as in any order: the key changes
-  // only together with the traveltime, in the neighbour's own visit.
-  uint8_t cd1[ND][2], cd2[ND][2];
-  double t2[ND][2];
-  long long l2[ND][2];
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      const int sh = s == 0 ? 1 : -1;
-      l2[ax][s] = -1;
-      if (l1[ax][s] < 0) continue;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += sh;
-      bool ok = true;  // isonbord on the first neighbour, in every coordinate (eikutils.jl:129-162)
-#pragma unroll
-      for (int dd = 0; dd < ND; dd++)
-        if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
-      if (ok) {
-        p[ax] += sh;
-        l2[ax][s] = lin3(g, p[0], p[1], p[2]);
-      }
-    }
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      cd1[ax][s] = l1[ax][s] >= 0 ? __ldcg(P.code + l1[ax][s]) : (uint8_t)0;
-      t2[ax][s] = l2[ax][s] >= 0 ? __ldcg(P.t + l2[ax][s]) : EIK_INF;
-      cd2[ax][s] = l2[ax][s] >= 0 ? __ldcg(P.code + l2[ax][s]) : (uint8_t)0;
-    }
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      if (l1[ax][s] < 0) continue;
-      double L;
-      int d;
-      node_key(P, l1[ax][s], t1[ax][s], cd1[ax][s], &L, &d);
-      nb_put1(nb, ax, s, t1[ax][s], L, d);
-      if (l2[ax][s] >= 0) {
-        node_key(P, l2[ax][s], t2[ax][s], cd2[ax][s], &L, &d);
-        nb_put2(nb, ax, s, t2[ax][s], L, d);
-      }
-    }
-  int8_t cd[3] = {0, 0, 0};
-  Key nk;
-  bool neg = false;
-  PL_T(tq2);
-  const double nv = prefix_rule<ND>(nb, cd, &nk, &neg);
-  PL_ADD(9, tq2);
-  (*evals)++;
-  const uint8_t nc = pack_codes(cd, ND);
-  const bool same_t = (nv == told) || (isinf(nv) && isinf(told));
-  const bool tkchange = !(same_t && key_eq(nk, Key{Lold, dold, told}));
-  const bool special = !(nk.L == nv && nk.d == 0);
-  const uint8_t ncb = (uint8_t)(nc | (special ? CODE_SRC_BIT : 0));
-  a.rs.tent[gbase + l] = nv;
-  if (!tkchange) {
-    if (ncb != cb) P.code[l] = ncb;
-    vk[5]++;
-    return 0;
-  }
-  if (nv > T) {  // not final yet: keep the old value and come back when the front is there
-    *front = nv;
-    vk[4]++;
-    return 1u << DIR_SELF;
-  }
-  P.t[l] = nv;
-  P.code[l] = ncb;
-  if (special) {
-    P.kL[l] = nk.L;
-    P.kd[l] = (uint8_t)nk.d;
-  }
-  __threadfence();
-  PL_T(tq3);
-  // The nodes whose stencil reads this one (+-1, +-2 along each axis) are evaluated again,
-  // except those whose stored key is at most both the old and the new key of this node:
-  // the order rule of such a node never accepts this one, nor is its termination test
-  // affected, so its value cannot change. A node listed for the current round may be
-  // under evaluation right now and is always listed again. The node two steps away reads
-  // this one only through the node in between, which must be reached first; when it is,
-  // its own change lists that node.
-  //
-  // Reads per axis in one batch, all after the fence above: the in-between node's
-  // traveltime (the +-1 node's, read fresh), and the stamp, traveltime and code of each
-  // candidate. A candidate whose stamp is below r is in no list of this round, so nothing
-  // writes its traveltime, code or key while this round runs: reading them before or after
-  // the stamp observes the same values.
-  const Key kold = Key{Lold, dold, told};
-  unsigned dirs = 0;
-#pragma unroll
-  for (int ax = 0; ax < ND; ax++) {
-    long long lj[4];
-    double tj[4];
-    uint8_t cj[4];
-    int32_t sj[4];
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int off = dir_off(j);
-      lj[j] = -1;
-      if (c[ax] + off < 0 || c[ax] + off >= g.n[ax]) continue;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += off;
-      lj[j] = lin3(g, p[0], p[1], p[2]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      tj[j] = lj[j] >= 0 ? __ldcg(P.t + lj[j]) : EIK_INF;
-      cj[j] = lj[j] >= 0 ? __ldcg(P.code + lj[j]) : (uint8_t)0;
-      sj[j] = lj[j] >= 0 ? *(volatile const int32_t*)(a.rs.stamp + gbase + lj[j]) : 0;
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      if (lj[j] < 0) continue;
-      // j = 0 (-2) reads this node through j = 1 (-1), j = 3 (+2) through j = 2 (+1)
-      if (j == 0 && !(tj[1] < EIK_INF)) continue;
-      if (j == 3 && !(tj[2] < EIK_INF)) continue;
-      if (sj[j] < r) {
-        double Lj;
-        int dj;
-        node_key(P, lj[j], tj[j], cj[j], &Lj, &dj);
-        const Key kj = Key{Lj, dj, tj[j]};
-        if (key_le(kj, kold) && key_le(kj, nk)) continue;
-      }
-      a.rs.dirty[gbase + lj[j]] = 1;
-      dirs |= 1u << (4 * ax + j);
-    }
-  }
-  *front = nv + P.incmin;  // no node reading this one can get a smaller value from it
-  PL_ADD(10, tq3);
-  PL_ADD(8, tq1);
-  vk[6]++;
-  return dirs;
 }
 
 // Forward coarse solve in rounds (one cooperative launch for all problems). Round r takes
@@ -484,8 +239,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
             const CoarseProblem& P = a.probs[prob];
             const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
             const unsigned long long gb = (unsigned long long)prob * N;
-            dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
-                             : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
+            dirs = (ND == 3) ? process_node<3>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk)
+                             : process_node<2>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk);
           }
           qn -= k;
           __syncwarp();
@@ -583,8 +338,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
             dirs = 1u << DIR_SELF;
             vk[0]++;
           } else {
-            dirs = (ND == 3) ? process_node<3>(a, P, gb, l, T, r, &front, &evals, vk)
-                             : process_node<2>(a, P, gb, l, T, r, &front, &evals, vk);
+            dirs = (ND == 3) ? process_node<3>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk)
+                             : process_node<2>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk);
           }
         }
         __syncwarp();

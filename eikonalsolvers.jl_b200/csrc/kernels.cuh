@@ -131,6 +131,13 @@ void launch_fine_replay(const ForwardBatch& fb, const uint8_t* fine_tie, cudaStr
 // ctas_per_sm: resident CTAs per SM of the persistent launch (0 = as many as fit);
 // queue: per-warp evaluation queue 1 = on, 0 = off, -1 = chosen by the launch's size
 cudaError_t launch_coarse_solve(const SolveArgs& sa, int nsm, int ctas_per_sm, int queue, cudaStream_t st);
+// The forward solve of small problems (every problem at most nmax nodes), one thread-block
+// cluster per problem with its state in distributed shared memory, seeds and counters
+// included (it replaces round init, seeding and launch_coarse_solve). *used = false when no
+// cluster of this GPU holds such a problem (nothing launched: use the global solve).
+cudaError_t launch_cluster_solve(const SolveArgs& sa, long long nmax, const int32_t* seed_lin, const double* seed_tt,
+                                 const SrcOut* out, bool fine_corners, int seedcap, cudaStream_t st, bool* used);
+bool cluster_solve_fits(const SolveArgs& sa, long long nmax);
 void launch_picks(const GridDesc& g, const double* t, long long N, int nsrc, const long long* recoff,
                   const double* rec, double* picks, cudaStream_t st);
 // Gaussian smoothing of a gradient field (smoothgradkern = l, odd): weights on the host,

@@ -1,0 +1,337 @@
+// One node visit of the forward round solver (coarse.cu, cluster.cu): the FMM order rule
+// of stencil.cuh evaluated on a node of one problem, with the gates, the write-back and the
+// relisting filter around it. The state it reads and writes is reached through an accessor
+// (M), so that the same visit runs on state in global memory and on state in a cluster's
+// distributed shared memory.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace eik {
+
+#ifdef EIK_PHASE
+#define PL_T(v) const long long v = clock64()
+#define PL_ADD(k, t0) vk[k] += (unsigned long long)(clock64() - (t0))
+#else
+#define PL_T(v)
+#define PL_ADD(k, t0)
+#endif
+
+// ------------------------------------------------------------------ node solve --
+// Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise.
+__device__ __forceinline__ void node_key(const CoarseProblem& P, long long l, double t, uint8_t cb, double* L, int* d) {
+  if (cb & CODE_SRC_BIT) {
+    *L = __ldcg(P.kL + l);
+    *d = __ldcg(P.kd + l);
+  } else {
+    *L = t;
+    *d = 0;
+  }
+}
+
+// Neighbour directions of a node: k = 4*axis + {0: -2, 1: -1, 2: +1, 3: +2}; bit 12 = itself.
+constexpr int DIR_SELF = 12;
+__device__ __forceinline__ int dir_off(int k) { return (k & 3) < 2 ? (k & 3) - 2 : (k & 3) - 1; }
+
+// The round-solver state of problem P in global memory: node l at l (problem arrays) and at
+// gb + l (round-solver arrays, numbered over the problems of a launch).
+struct GlobalNodes {
+  const SolveArgs& a;
+  const CoarseProblem& P;
+  unsigned long long gb;
+  __device__ __forceinline__ uint8_t dirty(long long l) const { return __ldcg(a.rs.dirty + gb + l); }
+  __device__ __forceinline__ void set_dirty(long long l, uint8_t v) const { a.rs.dirty[gb + l] = v; }
+  __device__ __forceinline__ double tent(long long l) const { return __ldcg(a.rs.tent + gb + l); }
+  __device__ __forceinline__ void set_tent(long long l, double v) const { a.rs.tent[gb + l] = v; }
+  __device__ __forceinline__ uint8_t code(long long l) const { return __ldcg(P.code + l); }
+  __device__ __forceinline__ void set_code(long long l, uint8_t v) const { P.code[l] = v; }
+  __device__ __forceinline__ double t(long long l) const { return __ldcg(P.t + l); }
+  __device__ __forceinline__ void set_t(long long l, double v) const { P.t[l] = v; }
+  __device__ __forceinline__ int32_t stamp(long long l) const {
+    return *(volatile const int32_t*)(a.rs.stamp + gb + l);
+  }
+  __device__ __forceinline__ void fence() const { __threadfence(); }
+};
+
+// The order rule on a neighbourhood with special keys (source points, non-causal
+// acceptances): the full keys of the immediate and distance-2 neighbours (arrays indexed
+// 2*axis + side; l < 0 where there is no such node). Kept out of line: it is rare, and its
+// key registers would otherwise weigh on every visit.
+template <int ND>
+__device__ __noinline__ double rule_full(const CoarseProblem& P, const long long* l1, const long long* l2,
+                                         const double* t1, const double* t2, const uint8_t* cd1, const uint8_t* cd2,
+                                         const double* dh, double slow, int8_t* cd, Key* nk, bool* neg) {
+  Nbhd nb;
+  nb_clear(nb);
+  for (int ax = 0; ax < 3; ax++) nb.dh[ax] = dh[ax];
+  nb.slow = slow;
+  nb.c1u = P.c1u;
+  nb.c2u = P.c2u;
+  for (int ax = 0; ax < ND; ax++)
+    for (int s = 0; s < 2; s++) {
+      const int k = 2 * ax + s;
+      if (l1[k] < 0) continue;
+      double L;
+      int d;
+      node_key(P, l1[k], t1[k], cd1[k], &L, &d);
+      nb_put1(nb, ax, s, t1[k], L, d);
+      if (l2[k] >= 0) {
+        node_key(P, l2[k], t2[k], cd2[k], &L, &d);
+        nb_put2(nb, ax, s, t2[k], L, d);
+      }
+    }
+  return prefix_rule<ND>(nb, cd, nk, neg);
+}
+
+// One listed node: gate, evaluate, write back. Returns the directions of the nodes to list
+// for the next round (bit DIR_SELF: this node again) and, in *front, the traveltime that
+// bounds their next evaluation from below. M holds the problem's round-solver state (the
+// node's traveltime, code, cached front, dirty flag and round stamp): global memory
+// (GlobalNodes) or the distributed shared memory of a thread-block cluster; key levels and
+// depths of special nodes and the slowness stay in global memory.
+//
+// The visit is a chain of dependent L2 round trips, which sets the length of a round when
+// fronts are small. Each stage therefore issues all of its loads before it uses any: the
+// node's own state, its immediate neighbours, their codes with the distance-2 nodes, and
+// the relist filter's reads per axis. Reordering these reads does not change what they
+// can observe (see the notes at each stage).
+template <int ND, class M>
+__device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem& P, long long l, double T, int r,
+                                                 double* front, unsigned long long* evals, unsigned long long* vk) {
+  PL_T(tq0);
+  const GridDesc& g = P.g;
+  const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
+  // The node's own state in one batch. Only this visit writes its t, code and key during
+  // the round (a node is listed once per round), so their order of reading is free.
+  const uint8_t dirty0 = m.dirty(l);
+  const double tv = m.tent(l);
+  const uint8_t cb = m.code(l);
+  const double told = m.t(l);
+  // last evaluated value, still valid while nothing the node reads has changed
+  if (!dirty0 && tv > T && tv < EIK_INF) {
+    *front = tv;
+    vk[0]++;
+    return 1u << DIR_SELF;
+  }
+  double Lold;
+  int dold;
+  node_key(P, l, told, cb, &Lold, &dold);
+  if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) {  // source points are fixed
+    vk[1]++;
+    return 0;
+  }
+  // from here the node reads its neighbours' current values: a change after this point
+  // marks it dirty again (writers store the value, fence, then the flag)
+  m.set_dirty(l, 0);
+  m.fence();
+  // immediate neighbours (one batch with the slowness): potential = smallest traveltime
+  double t1[ND][2];
+  long long l1[ND][2];
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int sh = s == 0 ? 1 : -1;
+      l1[ax][s] = -1;
+      if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      l1[ax][s] = lin3(g, p[0], p[1], p[2]);
+    }
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) t1[ax][s] = l1[ax][s] >= 0 ? m.t(l1[ax][s]) : EIK_INF;
+  const double slow = __ldg(P.slow + l);
+  double pot = EIK_INF;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) pot = fmin(pot, t1[ax][s]);
+  if (!(pot < EIK_INF)) {  // nothing reached around it yet
+    m.set_tent(l, EIK_INF);
+    vk[2]++;
+    return 0;
+  }
+  PL_ADD(7, tq0);
+  PL_T(tq1);
+  double dh[3];
+  node_dh(g, c[0], dh);
+  // Lower bound of the node's value: every term of the local update is at least pot and
+  // the quadratic adds at least (2/3) h s / sqrt(ND) (2nd-order coefficients 9/(4h^2)).
+  // Until the round threshold reaches it the node cannot be final: no evaluation yet.
+  double hmin = dh[0];
+#pragma unroll
+  for (int ax = 1; ax < ND; ax++) hmin = fmin(hmin, dh[ax]);
+  const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
+  if (lb > T) {
+    m.set_tent(l, lb);  // stands, like an evaluated value, while the node stays clean
+    *front = lb;
+    vk[3]++;
+    return 1u << DIR_SELF;
+  }
+  // Codes of the immediate neighbours and the distance-2 nodes with their codes, one batch.
+  // A neighbour's key is read after its traveltime here as in any order: the key changes
+  // only together with the traveltime, in the neighbour's own visit.
+  uint8_t cd1[ND][2], cd2[ND][2];
+  double t2[ND][2];
+  long long l2[ND][2];
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      const int sh = s == 0 ? 1 : -1;
+      l2[ax][s] = -1;
+      if (l1[ax][s] < 0) continue;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      bool ok = true;  // isonbord on the first neighbour, in every coordinate (eikutils.jl:129-162)
+#pragma unroll
+      for (int dd = 0; dd < ND; dd++)
+        if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
+      if (ok) {
+        p[ax] += sh;
+        l2[ax][s] = lin3(g, p[0], p[1], p[2]);
+      }
+    }
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      cd1[ax][s] = l1[ax][s] >= 0 ? m.code(l1[ax][s]) : (uint8_t)0;
+      t2[ax][s] = l2[ax][s] >= 0 ? m.t(l2[ax][s]) : EIK_INF;
+      cd2[ax][s] = l2[ax][s] >= 0 ? m.code(l2[ax][s]) : (uint8_t)0;
+    }
+  // Without a special key among them (the common case) every key is the traveltime: the
+  // rule runs on traveltimes alone (prefix_rule_plain), else on the full keys (rule_full).
+  bool plain = true;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      if (l1[ax][s] >= 0 && (cd1[ax][s] & CODE_SRC_BIT)) plain = false;
+      if (l2[ax][s] >= 0 && (cd2[ax][s] & CODE_SRC_BIT)) plain = false;
+    }
+  int8_t cd[3] = {0, 0, 0};
+  Key nk;
+  bool neg = false;
+  PL_T(tq2);
+  double nv;
+  if (plain) {
+    NbhdT nb;
+    nb.in1 = nb.ok2 = 0u;
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++)
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        nb.t1[ax][s] = EIK_INF;
+        nb.t2[ax][s] = EIK_INF;
+      }
+#pragma unroll
+    for (int ax = 0; ax < ND; ax++)
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        if (l1[ax][s] < 0) continue;
+        nb.t1[ax][s] = t1[ax][s];
+        nb.in1 |= 1u << slot(ax, s);
+        if (l2[ax][s] >= 0) {
+          nb.t2[ax][s] = t2[ax][s];
+          nb.ok2 |= 1u << slot(ax, s);
+        }
+      }
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) nb.dh[ax] = dh[ax];
+    nb.slow = slow;
+    nb.c1u = P.c1u;
+    nb.c2u = P.c2u;
+    nv = prefix_rule_plain<ND>(nb, cd, &nk, &neg);
+  } else {
+    nv = rule_full<ND>(P, &l1[0][0], &l2[0][0], &t1[0][0], &t2[0][0], &cd1[0][0], &cd2[0][0], dh, slow, cd, &nk, &neg);
+  }
+  PL_ADD(9, tq2);
+  (*evals)++;
+  const uint8_t nc = pack_codes(cd, ND);
+  const bool same_t = (nv == told) || (isinf(nv) && isinf(told));
+  const bool tkchange = !(same_t && key_eq(nk, Key{Lold, dold, told}));
+  const bool special = !(nk.L == nv && nk.d == 0);
+  const uint8_t ncb = (uint8_t)(nc | (special ? CODE_SRC_BIT : 0));
+  m.set_tent(l, nv);
+  if (!tkchange) {
+    if (ncb != cb) m.set_code(l, ncb);
+    vk[5]++;
+    return 0;
+  }
+  if (nv > T) {  // not final yet: keep the old value and come back when the front is there
+    *front = nv;
+    vk[4]++;
+    return 1u << DIR_SELF;
+  }
+  m.set_t(l, nv);
+  m.set_code(l, ncb);
+  if (special) {
+    P.kL[l] = nk.L;
+    P.kd[l] = (uint8_t)nk.d;
+  }
+  m.fence();
+  PL_T(tq3);
+  // The nodes whose stencil reads this one (+-1, +-2 along each axis) are evaluated again,
+  // except those whose stored key is at most both the old and the new key of this node:
+  // the order rule of such a node never accepts this one, nor is its termination test
+  // affected, so its value cannot change. A node listed for the current round may be
+  // under evaluation right now and is always listed again. The node two steps away reads
+  // this one only through the node in between, which must be reached first; when it is,
+  // its own change lists that node.
+  //
+  // Reads per axis in one batch, all after the fence above: the in-between node's
+  // traveltime (the +-1 node's, read fresh), and the stamp, traveltime and code of each
+  // candidate. A candidate whose stamp is below r is in no list of this round, so nothing
+  // writes its traveltime, code or key while this round runs: reading them before or after
+  // the stamp observes the same values.
+  const Key kold = Key{Lold, dold, told};
+  unsigned dirs = 0;
+#pragma unroll
+  for (int ax = 0; ax < ND; ax++) {
+    long long lj[4];
+    double tj[4];
+    uint8_t cj[4];
+    int32_t sj[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int off = dir_off(j);
+      lj[j] = -1;
+      if (c[ax] + off < 0 || c[ax] + off >= g.n[ax]) continue;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += off;
+      lj[j] = lin3(g, p[0], p[1], p[2]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      tj[j] = lj[j] >= 0 ? m.t(lj[j]) : EIK_INF;
+      cj[j] = lj[j] >= 0 ? m.code(lj[j]) : (uint8_t)0;
+      sj[j] = lj[j] >= 0 ? m.stamp(lj[j]) : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      if (lj[j] < 0) continue;
+      // j = 0 (-2) reads this node through j = 1 (-1), j = 3 (+2) through j = 2 (+1)
+      if (j == 0 && !(tj[1] < EIK_INF)) continue;
+      if (j == 3 && !(tj[2] < EIK_INF)) continue;
+      if (sj[j] < r) {
+        double Lj;
+        int dj;
+        node_key(P, lj[j], tj[j], cj[j], &Lj, &dj);
+        const Key kj = Key{Lj, dj, tj[j]};
+        if (key_le(kj, kold) && key_le(kj, nk)) continue;
+      }
+      m.set_dirty(lj[j], 1);
+      dirs |= 1u << (4 * ax + j);
+    }
+  }
+  *front = nv + P.incmin;  // no node reading this one can get a smaller value from it
+  PL_ADD(10, tq3);
+  PL_ADD(8, tq1);
+  vk[6]++;
+  return dirs;
+}
+
+}  // namespace eik

@@ -158,6 +158,7 @@ struct eik_ctx {
   double round_gate = 0.0;  // forward round width in units of (smallest spacing x smallest slowness); 0 = by size
   int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
   int fwd_queue = -1;        // per-warp evaluation queue of the forward solve: -1 by size, 0 off, 1 on
+  int cluster_solve = 1;     // small problems solved in one thread-block cluster each (1) or globally (0)
   int max_rounds = 0;        // round limit of the persistent solves (0 = the library's: 2^24 forward)
   double sm_fraction = 0.0; // share of the SMs the persistent (cooperative) solves use; 0 = by size
   double ray_room = 3.0;     // room of a ray in its first tracing pass, in straight-line lengths

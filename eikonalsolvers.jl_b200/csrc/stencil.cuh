@@ -121,10 +121,30 @@ EIK_HD void nb_put2(Nbhd& nb, int a, int l, double t, double L, int d) {
   nb.ok2 |= 1u << slot(a, l);
 }
 
+// Acceptance by a group key T: the neighbour is in the grid (distance 1) or 2nd order is
+// allowed on that side (distance 2), and its key is at most T.
+EIK_HD bool acc1(const Nbhd& nb, int a, int l, const Key& T) { return nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T); }
+EIK_HD bool acc2(const Nbhd& nb, int a, int l, const Key& T) { return nb_ok2(nb, a, l) && key_le(nb_key2(nb, a, l), T); }
+
+// Neighbourhood in which no node (distance 1 or 2) has a special key: every key is
+// (t, 0, t), so a key is its traveltime and acceptance by the group key (tg, 0, tg) is
+// t <= tg (key_le of two such keys; tg is a reached neighbour's finite traveltime).
+struct NbhdT {
+  double t1[3][2];
+  double t2[3][2];
+  uint32_t in1, ok2;  // as in Nbhd
+  double dh[3];
+  double slow;
+  double c1u, c2u;
+};
+EIK_HD bool acc1(const NbhdT& nb, int a, int l, double tg) { return ((nb.in1 >> slot(a, l)) & 1u) && nb.t1[a][l] <= tg; }
+EIK_HD bool acc2(const NbhdT& nb, int a, int l, double tg) { return ((nb.ok2 >> slot(a, l)) & 1u) && nb.t2[a][l] <= tg; }
+
 // calcttpt_2ndord! with accepted(x) := key(x) <= T. codes receive the reference's
-// derivative codes (codeD): -side for 1st order, -2*side for 2nd order, 0 unused.
-template <int ND>
-EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdisc) {
+// derivative codes (codeD): -side for 1st order, -2*side for 2nd order, 0 unused. NB is a
+// neighbourhood (Nbhd with group keys, NbhdT with group traveltimes).
+template <int ND, class NB, class TK>
+EIK_HD double update_at_g(const NB& nb, const TK& T, int8_t* codes, bool* negdisc) {
   double alpha = 0.0, beta = 0.0, gamma = -(nb.slow * nb.slow);
 #pragma unroll
   for (int a = 0; a < ND; a++) codes[a] = 0;
@@ -135,13 +155,13 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
 #pragma unroll
     for (int l = 0; l < 2; l++) {
       const int sh = l == 0 ? 1 : -1;
-      if (nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T)) {
+      if (acc1(nb, a, l, T)) {
         const double tv1 = nb.t1[a][l];
         if (tv1 < cv1) {
           cv1 = tv1;
           use1 = true;
           codes[a] = (int8_t)(-sh);
-          if (nb_ok2(nb, a, l) && key_le(nb_key2(nb, a, l), T)) {
+          if (acc2(nb, a, l, T)) {
             const double tv2 = nb.t2[a][l];
             if (tv2 <= cv1) {
               cv2 = tv2;
@@ -183,7 +203,7 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
 #pragma unroll
       for (int l = 0; l < 2; l++) {
         const int sh = l == 0 ? 1 : -1;
-        if (nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T)) {
+        if (acc1(nb, a, l, T)) {
           const double tv1 = nb.t1[a][l];
           if (tv1 < cv1) {
             cv1 = tv1;
@@ -211,7 +231,7 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
 #pragma unroll
       for (int l = 0; l < 2; l++) {
         const int sh = l == 0 ? 1 : -1;
-        if (nb_in1(nb, a, l) && key_le(nb_key1(nb, a, l), T)) {
+        if (acc1(nb, a, l, T)) {
           const double tv1 = nb.t1[a][l];
           if (tv1 < cv[a]) {
             cv[a] = tv1;
@@ -241,6 +261,11 @@ EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdi
   // are monotone, so the '+' root is never below the '-' root: it is the larger one.
   const double tmpsq = sqrt(sqarg);
   return (-beta + tmpsq) / (2.0 * alpha);
+}
+
+template <int ND>
+EIK_HD double update_at(const Nbhd& nb, const Key& T, int8_t* codes, bool* negdisc) {
+  return update_at_g<ND>(nb, T, codes, negdisc);
 }
 
 // Smallest key of a reached in-grid immediate neighbour, strictly above lo if strict.
@@ -304,6 +329,50 @@ EIK_HD double prefix_rule(const Nbhd& nb, int8_t* codes, Key* key_out, bool* neg
     for (int a = 0; a < ND; a++) cprev[a] = cg[a];
     kg = kn;
     first = false;
+  }
+  *key_out = key_unreached();
+  return EIK_INF;
+}
+
+// prefix_rule on a neighbourhood without special keys (NbhdT): the groups are the distinct
+// traveltimes of the reached immediate neighbours in increasing order. A group never has a
+// depth, so the depth limit of prefix_rule never applies, and its own key is (v, 0, v) when
+// the value lies above the group, else (tg, 1, v), accepted right after the group. Same
+// value, codes and key as prefix_rule on the same neighbourhood written as an Nbhd.
+template <int ND>
+EIK_HD double prefix_rule_plain(const NbhdT& nb, int8_t* codes, Key* key_out, bool* negdisc) {
+#pragma unroll
+  for (int a = 0; a < ND; a++) codes[a] = 0;
+  double tg = EIK_INF;
+#pragma unroll
+  for (int a = 0; a < ND; a++)
+#pragma unroll
+    for (int l = 0; l < 2; l++)
+      if (((nb.in1 >> slot(a, l)) & 1u) && nb.t1[a][l] < tg) tg = nb.t1[a][l];
+  if (!(tg < EIK_INF)) {
+    *key_out = key_unreached();
+    return EIK_INF;
+  }
+#pragma unroll 1
+  for (int g = 0; g < 2 * ND; g++) {
+    int8_t cg[3];
+    const double v = update_at_g<ND>(nb, tg, cg, negdisc);
+#pragma unroll
+    for (int a = 0; a < ND; a++) codes[a] = cg[a];
+    double tn = EIK_INF;
+#pragma unroll
+    for (int a = 0; a < ND; a++)
+#pragma unroll
+      for (int l = 0; l < 2; l++) {
+        const double t = nb.t1[a][l];
+        if (((nb.in1 >> slot(a, l)) & 1u) && t > tg && t < tn) tn = t;
+      }
+    const bool above = v > tg;
+    if (!(tn < EIK_INF) || !above || v <= tn) {
+      *key_out = above ? key_normal(v) : Key{tg, 1, v};
+      return v;
+    }
+    tg = tn;
   }
   *key_out = key_unreached();
   return EIK_INF;

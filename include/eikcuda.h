@@ -135,8 +135,11 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * source instead of only where an exact tie decides its stop (default 0); "max_rounds" = round
  * limit of the persistent forward and adjoint solves, an integer, 0 (the default) = the
  * library's (2^24 forward, 2^26 adjoint); a solve that reaches it stops on the device and the
- * call returns EIK_ERR_NOT_CONVERGED, the context staying usable. Returns EIK_ERR_ASSERT for
- * an unknown name or a value out of range. */
+ * call returns EIK_ERR_NOT_CONVERGED, the context staying usable; "cluster_solve" = 1 (the
+ * default) solves problems small enough for one thread-block cluster's shared memory (the
+ * refined windows, grids up to ~95 000 nodes) with one cluster each, 0 always uses the
+ * persistent global solve. Returns EIK_ERR_ASSERT for an unknown name or a value out of
+ * range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 
 /* No counterpart in the reference: failure-detection self-test. Runs, on the context's
