@@ -1456,8 +1456,10 @@ extern "C" int eik_gradient(eik_ctx* ctx, eik_model_id model, int64_t nsrc, cons
     rc = gradient_chunked(ctx, m, nsrc, chunk, d_cs, rec_off, d_rec, d_po, d_so, whichgrad, ep,
                           wantvel ? d_gv : nullptr, wantsrc ? d_gs : nullptr, d_m, stats);
   else
-    rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
-                       wantsrc ? d_gs : nullptr, d_m, stats, nullptr);
+    rc = run_with_retry(ctx, stats, [&]() {
+      return gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
+                           wantsrc ? d_gs : nullptr, d_m, stats, nullptr);
+    });
   if (rc) return rc;
   double hm = 0.0;
   CUDA_OK(ctx, cudaMemcpyAsync(&hm, d_m, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1535,8 +1537,10 @@ extern "C" int eik_gradient_groups(eik_ctx* ctx, eik_model_id model, int64_t ngr
   }
   const bool wantvel = whichgrad == 1 || whichgrad == 3, wantsrc = whichgrad != 1;
   const GroupSpec gsp{ngroups, group_off};
-  rc = gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
-                     wantsrc ? d_gs : nullptr, d_m, stats, nullptr, nullptr, &gsp);
+  rc = run_with_retry(ctx, stats, [&]() {
+    return gradient_core(ctx, m, nsrc, d_cs, d_off, d_rec, d_po, d_so, whichgrad, ep, wantvel ? d_gv : nullptr,
+                         wantsrc ? d_gs : nullptr, d_m, stats, nullptr, nullptr, &gsp);
+  });
   if (rc) return rc;
   if (misfit) CUDA_OK(ctx, cudaMemcpyAsync(misfit, d_m, sizeof(double) * ngroups, cudaMemcpyDeviceToHost, st));
   if (gradvel && wantvel)
@@ -1598,9 +1602,11 @@ extern "C" int eik_gradient_device(eik_ctx* ctx, eik_model_id model, int64_t nsr
     long long* d_off = (long long*)ctx->scratch.get("in_off", sizeof(long long) * (nsrc + 1), &rc);
     if (!d_off) return fail(ctx, rc, "scratch allocation failed");
     CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
-    rc = gradient_core(ctx, m, nsrc, coordsrc_dev, d_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad, ep,
-                       (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
-                       misfit_dev, stats, nullptr);
+    rc = run_with_retry(ctx, stats, [&]() {
+      return gradient_core(ctx, m, nsrc, coordsrc_dev, d_off, rec_dev, pickobs_dev, stdobs_dev, whichgrad, ep,
+                           (whichgrad != 2) ? gradvel_dev : nullptr, (whichgrad != 1) ? gradsrc_dev : nullptr,
+                           misfit_dev, stats, nullptr);
+    });
   }
   if (rc) return rc;
   cudaEventRecord(ctx->ev1, st);

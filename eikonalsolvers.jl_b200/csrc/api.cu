@@ -368,7 +368,22 @@ int forward_multi(eik_ctx* ctx, int nmod, const Model* const* models, const int6
     sa.rs.rounds = (int32_t*)(rc32 + 8);
     sa.rs.visits = reinterpret_cast<unsigned long long*>(rc32 + 12);  // 8-byte aligned: 7 counters
   }
-  sa.rs.max_rounds = ctx->max_rounds > 0 ? ctx->max_rounds : (1 << 24);
+  // round limit: the caller's, else 256 rounds per node of the grid's diameter (a solve
+  // takes 2-7 in practice) plus 65536, so that a schedule that fails to settle is stopped in
+  // seconds and the call re-run with another (run_with_retry); 2^24 on that re-run
+  auto round_limit = [&](long long diam) -> int {
+    if (ctx->max_rounds > 0) return ctx->max_rounds;
+    if (ctx->retry) return 1 << 24;
+    if (ctx->auto_round_limit > 0) return ctx->auto_round_limit;
+    return (int)std::min<long long>(1LL << 24, 256LL * diam + 65536);
+  };
+  long long diam = 0;
+  for (int i = 0; i < nmod; i++) {
+    long long d = 0;
+    for (int a = 0; a < nd; a++) d += models[i]->g.n[a];
+    diam = std::max(diam, d);
+  }
+  sa.rs.max_rounds = round_limit(diam);
   sa.rs.stride = (unsigned long long)N;
   sa.err = fb.err;
   sa.probs = dp;
@@ -452,6 +467,7 @@ int forward_multi(eik_ctx* ctx, int nmod, const Model* const* models, const int6
     fsa.rs.stride = (unsigned long long)fb.nfmax;
     fsa.activations = sa.activations + 6;  // own counters: the coarse solve's stay separate
     fsa.node_evals = sa.activations + 7;
+    fsa.rs.max_rounds = round_limit((long long)nd * ((2LL * ep.noderadius + 1) * ep.downscalefactor + 1));
     // the windows are small: one thread-block cluster each when the GPU has room for it
     bool in_cluster = false;
     if (ctx->cluster_solve)
@@ -654,6 +670,12 @@ int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value) {
     ctx->fwd_queue = (int)value;
     return EIK_OK;
   }
+  if (std::strcmp(name, "auto_round_limit") == 0) {
+    if (!(value >= 0.0 && value <= (double)(1 << 24) && value == (double)(long long)value))
+      return fail(ctx, EIK_ERR_ASSERT, "auto_round_limit must be an integer in [0, 2^24] (0 = by the grid's size)");
+    ctx->auto_round_limit = (int)value;
+    return EIK_OK;
+  }
   if (std::strcmp(name, "cluster_solve") == 0) {
     if (!(value == 0.0 || value == 1.0)) return fail(ctx, EIK_ERR_ASSERT, "cluster_solve must be 0 or 1");
     ctx->cluster_solve = (int)value;
@@ -778,17 +800,19 @@ int eik_traveltime(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const double*
   CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemcpyAsync(d_off, rec_off, sizeof(long long) * (nsrc + 1), cudaMemcpyHostToDevice, st));
   if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
-  ForwardState fw;
-  rc = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
-  if (rc) return rc;
-  if (nrec) launch_picks(m.g, fw.t, m.N, (int)nsrc, d_off, d_rec, d_picks, st);
-  if (nrec && stats) stats->launches += 1;
-  CUDA_OK(ctx, cudaGetLastError());
-  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
-  if (ttgrids)
-    CUDA_OK(ctx, cudaMemcpyAsync(ttgrids, fw.t, sizeof(double) * nsrc * m.N, cudaMemcpyDeviceToHost, st));
-  cudaEventRecord(ctx->ev1, st);
-  rc = collect_forward_stats(ctx, &fw, stats);
+  rc = run_with_retry(ctx, stats, [&]() -> int {
+    ForwardState fw;
+    int r = forward_device(ctx, m, nsrc, d_cs, ep, &fw, stats);
+    if (r) return r;
+    if (nrec) launch_picks(m.g, fw.t, m.N, (int)nsrc, d_off, d_rec, d_picks, st);
+    if (nrec && stats) stats->launches += 1;
+    CUDA_OK(ctx, cudaGetLastError());
+    if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
+    if (ttgrids)
+      CUDA_OK(ctx, cudaMemcpyAsync(ttgrids, fw.t, sizeof(double) * nsrc * m.N, cudaMemcpyDeviceToHost, st));
+    cudaEventRecord(ctx->ev1, st);
+    return collect_forward_stats(ctx, &fw, stats);
+  });
   if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -853,32 +877,34 @@ int eik_traveltime_multi(eik_ctx* ctx, int64_t nmodel, const eik_model_id* model
   CUDA_OK(ctx, cudaMemcpyAsync(d_cs, coordsrc, sizeof(double) * nsrc * nd, cudaMemcpyHostToDevice, st));
   CUDA_OK(ctx, cudaMemcpyAsync(d_off, rel_src, sizeof(int64_t) * rel.size(), cudaMemcpyHostToDevice, st));
   if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(d_rec, rec, sizeof(double) * nrec * nd, cudaMemcpyHostToDevice, st));
-  ForwardState fw;
-  rc = forward_multi(ctx, (int)nmodel, mods.data(), src_off, d_cs, ep, &fw, stats);
-  if (rc) return rc;
-  for (int64_t i = 0; i < nmodel; i++) {
-    const int64_t o = src_off[i], n = src_off[i + 1] - o;
-    if (n == 0 || rec_off[o + n] == rec_off[o]) continue;
-    launch_picks(mods[i]->g, fw.t + o * fw.N, fw.N, (int)n, d_off + o + i, d_rec + rec_off[o] * nd,
-                 d_picks + rec_off[o], st);
-    if (stats) stats->launches += 1;
-  }
-  CUDA_OK(ctx, cudaGetLastError());
-  if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
-  if (ttgrids) {
-    // each source's grid at its own size, one after another
-    double* dst = ttgrids;
+  rc = run_with_retry(ctx, stats, [&]() -> int {
+    ForwardState fw;
+    int r = forward_multi(ctx, (int)nmodel, mods.data(), src_off, d_cs, ep, &fw, stats);
+    if (r) return r;
     for (int64_t i = 0; i < nmodel; i++) {
       const int64_t o = src_off[i], n = src_off[i + 1] - o;
-      if (n == 0) continue;
-      const size_t w = sizeof(double) * (size_t)mods[i]->N;
-      CUDA_OK(ctx, cudaMemcpy2DAsync(dst, w, fw.t + o * fw.N, sizeof(double) * (size_t)fw.N, w, (size_t)n,
-                                     cudaMemcpyDeviceToHost, st));
-      dst += n * mods[i]->N;
+      if (n == 0 || rec_off[o + n] == rec_off[o]) continue;
+      launch_picks(mods[i]->g, fw.t + o * fw.N, fw.N, (int)n, d_off + o + i, d_rec + rec_off[o] * nd,
+                   d_picks + rec_off[o], st);
+      if (stats) stats->launches += 1;
     }
-  }
-  cudaEventRecord(ctx->ev1, st);
-  rc = collect_forward_stats(ctx, &fw, stats);
+    CUDA_OK(ctx, cudaGetLastError());
+    if (nrec) CUDA_OK(ctx, cudaMemcpyAsync(picks, d_picks, sizeof(double) * nrec, cudaMemcpyDeviceToHost, st));
+    if (ttgrids) {
+      // each source's grid at its own size, one after another
+      double* dst = ttgrids;
+      for (int64_t i = 0; i < nmodel; i++) {
+        const int64_t o = src_off[i], n = src_off[i + 1] - o;
+        if (n == 0) continue;
+        const size_t w = sizeof(double) * (size_t)mods[i]->N;
+        CUDA_OK(ctx, cudaMemcpy2DAsync(dst, w, fw.t + o * fw.N, sizeof(double) * (size_t)fw.N, w, (size_t)n,
+                                       cudaMemcpyDeviceToHost, st));
+        dst += n * mods[i]->N;
+      }
+    }
+    cudaEventRecord(ctx->ev1, st);
+    return collect_forward_stats(ctx, &fw, stats);
+  });
   if (stats) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);

@@ -159,7 +159,9 @@ struct eik_ctx {
   int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
   int fwd_queue = -1;        // per-warp evaluation queue of the forward solve: -1 by size, 0 off, 1 on
   int cluster_solve = 1;     // small problems solved in one thread-block cluster each (1) or globally (0)
-  int max_rounds = 0;        // round limit of the persistent solves (0 = the library's: 2^24 forward)
+  int max_rounds = 0;        // round limit of the persistent solves (0 = the library's, see forward_multi)
+  int retry = 0;             // a pipeline run again after the automatic round limit: wider rounds, limit 2^24
+  int auto_round_limit = 0;  // the automatic round limit of a first run (0 = by the grid's diameter)
   double sm_fraction = 0.0; // share of the SMs the persistent (cooperative) solves use; 0 = by size
   double ray_room = 3.0;     // room of a ray in its first tracing pass, in straight-line lengths
   bool fine_replay = false; // refined start-up by exact heap replay for every source (else only on ties)
@@ -168,7 +170,8 @@ struct eik_ctx {
   // by a grid barrier over all resident CTAs), so they take wider rounds on fewer SMs.
   static constexpr unsigned long long SMALL_WORK = 1ull << 22;
   double gate_for(unsigned long long work) const {
-    return round_gate > 0.0 ? round_gate : (work < SMALL_WORK ? 8.0 : 2.0);
+    const double g = round_gate > 0.0 ? round_gate : (work < SMALL_WORK ? 8.0 : 2.0);
+    return retry ? 1.5 * g : g;
   }
   int sms_for(unsigned long long work) const {
     const double f = sm_fraction > 0.0 ? sm_fraction : (work < SMALL_WORK ? 0.25 : 1.0);
@@ -184,3 +187,21 @@ struct eik_ctx {
   eik_model_id next_model = 0;
   std::map<eik_model_id, eik::Model> models;
 };
+
+namespace eik {
+// Runs one pipeline (`call`, which returns an EIK_* code); when its forward solve stopped at
+// the library's automatic round limit (no max_rounds set), runs it once more with wider
+// rounds and the full limit. The solve's result is the fixed point of the order rule, the
+// same under every schedule, so the second run gives what the first would have.
+template <class F>
+int run_with_retry(eik_ctx* ctx, eik_stats* stats, F call) {
+  int rc = call();
+  if (rc == EIK_ERR_NOT_CONVERGED && ctx->max_rounds == 0) {
+    ctx->retry = 1;
+    rc = call();
+    ctx->retry = 0;
+    if (stats) stats->retries += 1;
+  }
+  return rc;
+}
+}  // namespace eik

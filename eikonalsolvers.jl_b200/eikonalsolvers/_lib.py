@@ -74,7 +74,7 @@ class eik_stats(C.Structure):
                 ("node_evals", C.c_uint64), ("device_ms", C.c_double), ("fine_ms", C.c_double),
                 ("solve_ms", C.c_double), ("adj_ms", C.c_double), ("adj_rounds", C.c_uint64),
                 ("launches", C.c_uint64), ("fwd_rounds", C.c_uint64),
-                ("fine_replays", C.c_uint64), ("fwd_visits", C.c_uint64 * 7), ("chunks", C.c_uint64)]
+                ("fine_replays", C.c_uint64), ("fwd_visits", C.c_uint64 * 7), ("chunks", C.c_uint64), ("retries", C.c_uint64)]
 
 
 _lib = None

@@ -107,6 +107,7 @@ typedef struct {
                                 source point, nothing reached, bound above the front,
                                 evaluated above the front, evaluated unchanged, changed */
   uint64_t chunks;           /* gradient calls split to fit the HBM budget: pipelines run (else 0) */
+  uint64_t retries;          /* pipelines run again after the automatic round limit (see max_rounds) */
 } eik_stats;
 
 /* Fills the reference defaults of ExtraParams(). */
@@ -133,9 +134,13 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * the single tracing pass, in multiples of its straight-line length (default 3; rays that
  * outgrow it are traced again); "fine_replay" = 1 replays the refined start-up's heap for every
  * source instead of only where an exact tie decides its stop (default 0); "max_rounds" = round
- * limit of the persistent forward and adjoint solves, an integer, 0 (the default) = the
- * library's (2^24 forward, 2^26 adjoint); a solve that reaches it stops on the device and the
- * call returns EIK_ERR_NOT_CONVERGED, the context staying usable; "cluster_solve" = 1 (the
+ * limit of the persistent forward and adjoint solves, an integer; a solve that reaches it
+ * stops on the device and the call returns EIK_ERR_NOT_CONVERGED, the context staying usable.
+ * 0 (the default) = the library's: for a forward solve 256 rounds per node of its grid's
+ * diameter (the sum of its sizes) plus 65 536, and a call whose forward solve reaches that
+ * limit runs once more with wider rounds and a limit of 2^24 (eik_stats.retries; the result
+ * does not depend on the schedule), 2^26 for the adjoint; "auto_round_limit" = that
+ * automatic limit of a first run, an integer, 0 (the default) = by the grid's diameter; "cluster_solve" = 1 (the
  * default) solves problems small enough for one thread-block cluster's shared memory (the
  * refined windows, grids up to ~95 000 nodes) with one cluster each, 0 always uses the
  * persistent global solve. Returns EIK_ERR_ASSERT for an unknown name or a value out of

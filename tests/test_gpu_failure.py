@@ -85,3 +85,37 @@ def test_halfway_source_is_shifted_and_warned(ctx):
     op, warn = O.eiktraveltime(vel, grd, cs, rec, extraparams=ExtraParams(), return_warn=True)
     assert warn & 0x2
     assert np.array_equal(picks[0], op[0])
+
+
+def test_automatic_round_limit_reruns_the_call():
+    """A forward solve that stops at the automatic round limit (no max_rounds set) is run
+    once more with wider rounds and the full limit: the call succeeds, bit-identical to the
+    oracle, and eik_stats.retries says so; with max_rounds set the limit is a hard stop."""
+    import eikoracle as O
+    from eikonalsolvers import Context
+    from eikonalsolvers import configs as CF
+    c = Context(0)
+    try:
+        w = CF.cfg1()
+        mid = c.upload(w.vel, w.grd)
+        op = O.eiktraveltime(w.vel, w.grd, w.coordsrc, w.coordrec, extraparams=w.extraparams)
+        for cl in (1.0, 0.0):
+            c.set_param("cluster_solve", cl)
+            c.set_param("auto_round_limit", 5)
+            pk = c.traveltime(mid, w.grd, w.coordsrc, w.coordrec)
+            assert c.last_stats.retries == 1
+            assert all(np.array_equal(a, b) for a, b in zip(pk, op))
+            c.set_param("auto_round_limit", 0)
+            c.traveltime(mid, w.grd, w.coordsrc, w.coordrec)
+            assert c.last_stats.retries == 0
+        po = [p + 0.01 for p in op]
+        so = [0.01 * np.ones(p.shape) for p in op]
+        g0 = c.gradient(mid, w.grd, w.coordsrc, w.coordrec, po, so, "gradvel")
+        c.set_param("auto_round_limit", 5)
+        g1 = c.gradient(mid, w.grd, w.coordsrc, w.coordrec, po, so, "gradvel")
+        assert c.last_stats.retries == 1
+        assert np.array_equal(g0[0], g1[0]) and g0[1] == g1[1]
+        c.set_param("auto_round_limit", 0)
+        c.release(mid)
+    finally:
+        c.close()
