@@ -158,7 +158,7 @@ struct eik_ctx {
   double round_gate = 0.0;  // forward round width in units of (smallest spacing x smallest slowness); 0 = by size
   int ctas_per_sm = 0;       // resident CTAs per SM of the forward solve (0 = as many as fit)
   int fwd_queue = -1;        // per-warp evaluation queue of the forward solve: -1 by size, 0 off, 1 on
-  int cluster_solve = 1;     // small problems solved in one thread-block cluster each (1) or globally (0)
+  int cluster_solve = 1;     // small problems in one thread-block cluster each: 1 in 2D, 2 in any dimension, 0 never
   int max_rounds = 0;        // round limit of the persistent solves (0 = the library's, see forward_multi)
   int retry = 0;             // a pipeline run again after the automatic round limit: wider rounds, limit 2^24
   int auto_round_limit = 0;  // the automatic round limit of a first run (0 = by the grid's diameter)

@@ -140,10 +140,10 @@ void* eik_ctx_stream(eik_ctx* ctx);
  * diameter (the sum of its sizes) plus 65 536, and a call whose forward solve reaches that
  * limit runs once more with wider rounds and a limit of 2^24 (eik_stats.retries; the result
  * does not depend on the schedule), 2^26 for the adjoint; "auto_round_limit" = that
- * automatic limit of a first run, an integer, 0 (the default) = by the grid's diameter; "cluster_solve" = 1 (the
- * default) solves problems small enough for one thread-block cluster's shared memory (the
- * refined windows, grids up to ~95 000 nodes) with one cluster each, 0 always uses the
- * persistent global solve. Returns EIK_ERR_ASSERT for an unknown name or a value out of
+ * automatic limit of a first run, an integer, 0 (the default) = by the grid's diameter; "cluster_solve" = how problems
+ * small enough for one thread-block cluster's shared memory (the refined windows, grids up to
+ * ~97 000 nodes) are solved: 1 (the default) = 2D ones in one cluster each (faster there),
+ * 2 = in any dimension, 0 = always the persistent global solve. Returns EIK_ERR_ASSERT for an unknown name or a value out of
  * range. */
 int eik_ctx_set_param(eik_ctx* ctx, const char* name, double value);
 

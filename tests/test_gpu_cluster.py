@@ -1,11 +1,11 @@
 """The forward solve of small problems in one thread-block cluster each (state in
 distributed shared memory, rounds separated by the cluster barrier) against the persistent
 global solve: picks, traveltime grids and gradients bit-identical with the context parameter
-cluster_solve on and off, for the refined windows (always small) and for coarse grids that
+cluster_solve forced on (2: any dimension) and off, for the refined windows (always small) and for coarse grids that
 fit a cluster, on 2D and 3D Cartesian and spherical grids. The oracle parity of the default
 path, which now takes the cluster solve on these sizes, is in test_gpu_forward.py and
 test_gpu_gradient.py. A round limit stops the cluster solve with EIK_ERR_NOT_CONVERGED and
-leaves the context usable."""
+leaves the context usable. By default (1) only 2D problems take the cluster."""
 import numpy as np
 import pytest
 
@@ -33,7 +33,7 @@ def ctx():
 
 
 def _tt(ctx, w, ep, on):
-    ctx.set_param("cluster_solve", 1.0 if on else 0.0)
+    ctx.set_param("cluster_solve", 2.0 if on else 0.0)
     mid = ctx.upload(w.vel, w.grd)
     try:
         return ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec, returntt=True, extraparams=ep), ctx.last_stats.launches
@@ -74,7 +74,7 @@ def test_cluster_solve_gradients_equal_global_solve(ctx, name, which):
     mid = ctx.upload(w.vel, w.grd)
     try:
         out = []
-        for on in (1.0, 0.0):
+        for on in (2.0, 0.0):
             ctx.set_param("cluster_solve", on)
             out.append(ctx.gradient(mid, w.grd, w.coordsrc, w.coordrec, po, so, which))
     finally:
@@ -102,3 +102,20 @@ def test_cluster_solve_round_limit(ctx):
     finally:
         ctx.set_param("max_rounds", 0)
         ctx.release(mid)
+
+
+def test_default_takes_clusters_in_2d_only(ctx):
+    w2, w3 = CF.cfg1(), CF.cfg3(scale=0.125, nsrc=3, nrec_side=4)
+    launches = {}
+    for name, w in (("2d", w2), ("3d", w3)):
+        for mode in (1.0, 0.0):
+            ctx.set_param("cluster_solve", mode)
+            mid = ctx.upload(w.vel, w.grd)
+            try:
+                ctx.traveltime(mid, w.grd, w.coordsrc, w.coordrec)
+                launches[name, mode] = ctx.last_stats.launches
+            finally:
+                ctx.release(mid)
+    ctx.set_param("cluster_solve", 1.0)
+    assert launches["2d", 1.0] < launches["2d", 0.0]
+    assert launches["3d", 1.0] == launches["3d", 0.0]
