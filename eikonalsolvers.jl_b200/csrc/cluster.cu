@@ -84,8 +84,19 @@ __device__ unsigned long long eik_cphase[8];
 extern "C" int eik_cphase_read(unsigned long long* out) {
   return (int)cudaMemcpyFromSymbol(out, eik_cphase, sizeof(unsigned long long) * 8);
 }
+// and, per round (first 4096), the largest per-warp time in each of phases 1-3 (the round's
+// critical warp)
+__device__ unsigned long long eik_cwarpmax[3][4096];
+extern "C" int eik_cwarpmax_read(unsigned long long* out) {
+  return (int)cudaMemcpyFromSymbol(out, eik_cwarpmax, sizeof(unsigned long long) * 3 * 4096);
+}
 #define CPH_T(v) const long long v = clock64()
-#define CPH_ADD(k, t0) if ((threadIdx.x & 31) == 0) atomicAdd(&eik_cphase[k], (unsigned long long)(clock64() - (t0)))
+#define CPH_ADD(k, t0)                                                                          \
+  {                                                                                             \
+    const unsigned long long dt_ = (unsigned long long)(clock64() - (t0));                      \
+    if ((threadIdx.x & 31) == 0) atomicAdd(&eik_cphase[k], dt_);                                \
+    if ((k) >= 1 && (k) <= 3) wsum_[(k) - 1] += dt_;                                           \
+  }
 #else
 #define CPH_T(v)
 #define CPH_ADD(k, t0)
@@ -181,6 +192,9 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
   int r = 0;
   for (; r < a.rs.max_rounds; r++) {
     const int b3 = r % 3, nb3 = (r + 1) % 3;
+#ifdef EIK_PHASE
+    unsigned long long wsum_[3] = {0, 0, 0};
+#endif
     CPH_T(tr0);
     // the cluster's entries and smallest pending front of this round: every CTA reduces the
     // same counters, read after the same barrier and written by no one this round (uniform)
@@ -258,6 +272,20 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
       __syncwarp();
       CPH_ADD(2, tp1);
       CPH_T(tp2);
+      // the owners' list slots in one batch of remote atomics, then the entries
+      unsigned int slot[DIR_SELF + 1];
+#pragma unroll
+      for (int k = 0; k <= DIR_SELF; k++) {
+        slot[k] = 0;
+        if (!((keep >> k) & 1u)) continue;
+        long long nl = l;
+        if (k != DIR_SELF) {
+          int pc[3] = {c[0], c[1], c[2]};
+          pc[k >> 2] += dir_off(k);
+          nl = lin3(g, pc[0], pc[1], pc[2]);
+        }
+        slot[k] = atomicAdd(&cl.map_shared_rank(&ctl, ClusterNodes<LGC>::rank_of(nl))->cnt[nb3], 1u);
+      }
 #pragma unroll
       for (int k = 0; k <= DIR_SELF; k++) {
         if (!((keep >> k) & 1u)) continue;
@@ -267,7 +295,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
           pc[k >> 2] += dir_off(k);
           nl = lin3(g, pc[0], pc[1], pc[2]);
         }
-        append(Lnext, nb3, nl, front);
+        cl.map_shared_rank(Lnext, ClusterNodes<LGC>::rank_of(nl))[slot[k]] = cluster_entry(nl, front);
       }
       __syncwarp();
       CPH_ADD(3, tp2);
@@ -279,6 +307,10 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
           fv < __longlong_as_double((long long)*(volatile const unsigned long long*)&ctl.nm[nb3]))
         atomicMin(&ctl.nm[nb3], (unsigned long long)__double_as_longlong(fv));
     }
+#ifdef EIK_PHASE
+    if (lane == 0 && r < 4096)
+      for (int k = 0; k < 3; k++) atomicMax(&eik_cwarpmax[k][r], wsum_[k]);
+#endif
     CPH_T(tb0);
     // this CTA's counters of round r+2 (last read in round r-1)
     if (threadIdx.x == 0) {
