@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/eikcuda.h"
+#include "node.cuh"
 #include "rounds.cuh"
 #include "runtime.hpp"
 
@@ -276,7 +277,8 @@ __device__ void adj_node(const AdjArgs& aa, int prob, long long l, unsigned long
   const AdjProblem& A = aa.ap[prob];
   const GridDesc& g = P.g;
   const long long N = npts(g);
-  const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
+  int c[3];
+  node_coords(g, l, c);
   long long nl[ND][4];
   uint8_t ncode[ND][4];
 #pragma unroll

@@ -182,11 +182,11 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
   }
   cl.sync();
 
-  unsigned long long evals = 0;
+  VisitCount evals = 0;
 #ifdef EIK_PHASE
-  unsigned long long vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles of the node visit
+  VisitCount vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles of the node visit
 #else
-  unsigned long long vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
+  VisitCount vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
 #endif
   double Tprev = -EIK_INF;
   int r = 0;
@@ -256,17 +256,11 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
       CPH_T(tp1);
       // list the next round's nodes once each (round stamps) with their owners; the stamp
       // exchanges go out together, then the appends
-      const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
       unsigned keep = 0;
 #pragma unroll
       for (int k = 0; k <= DIR_SELF; k++) {
         if (!((dirs >> k) & 1u)) continue;
-        long long nl = l;
-        if (k != DIR_SELF) {
-          int pc[3] = {c[0], c[1], c[2]};
-          pc[k >> 2] += dir_off(k);
-          nl = lin3(g, pc[0], pc[1], pc[2]);
-        }
+        const long long nl = dir_lin(g, l, k);
         if (atomicExch(m.at(s_stamp, nl), r + 1) != r + 1) keep |= 1u << k;
       }
       __syncwarp();
@@ -278,23 +272,13 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
       for (int k = 0; k <= DIR_SELF; k++) {
         slot[k] = 0;
         if (!((keep >> k) & 1u)) continue;
-        long long nl = l;
-        if (k != DIR_SELF) {
-          int pc[3] = {c[0], c[1], c[2]};
-          pc[k >> 2] += dir_off(k);
-          nl = lin3(g, pc[0], pc[1], pc[2]);
-        }
+        const long long nl = dir_lin(g, l, k);
         slot[k] = atomicAdd(&cl.map_shared_rank(&ctl, ClusterNodes<LGC>::rank_of(nl))->cnt[nb3], 1u);
       }
 #pragma unroll
       for (int k = 0; k <= DIR_SELF; k++) {
         if (!((keep >> k) & 1u)) continue;
-        long long nl = l;
-        if (k != DIR_SELF) {
-          int pc[3] = {c[0], c[1], c[2]};
-          pc[k >> 2] += dir_off(k);
-          nl = lin3(g, pc[0], pc[1], pc[2]);
-        }
+        const long long nl = dir_lin(g, l, k);
         cl.map_shared_rank(Lnext, ClusterNodes<LGC>::rank_of(nl))[slot[k]] = cluster_entry(nl, front);
       }
       __syncwarp();
@@ -333,8 +317,9 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
   }
   // counters: evaluations, visit outcomes, the largest round count
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
-  if (lane == 0 && evals) atomicAdd(a.node_evals, evals);
+  unsigned long long ev = evals;
+  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
+  if (lane == 0 && ev) atomicAdd(a.node_evals, ev);
   for (int k = 0; k < 7; k++) {
     unsigned long long v = vk[k];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

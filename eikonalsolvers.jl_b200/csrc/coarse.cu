@@ -158,11 +158,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
   const int lane = threadIdx.x & 31;
   __shared__ unsigned long long wq[SOLVE_THREADS / 32][QUEUE ? 64 : 1];  // per-warp queue of entries to evaluate
   const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
-  unsigned long long evals = 0;
+  VisitCount evals = 0;
 #ifdef EIK_PHASE
-  unsigned long long vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles: gates, node path, rule, relist filter
+  VisitCount vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles: gates, node path, rule, relist filter
 #else
-  unsigned long long vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
+  VisitCount vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
 #endif
   int r = 0;
   for (; r < a.rs.max_rounds; r++) {
@@ -249,18 +249,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
         PH_T(ts);
         // list the next round's nodes once each (per-node round stamps)
         const CoarseProblem& P = a.probs[prob];
-        const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
-                          (int)(l / ((long long)P.g.n[0] * P.g.n[1]))};
         const unsigned long long gbase = (unsigned long long)prob * N;
         unsigned keep = 0;
         for (int k = 0; k <= DIR_SELF; k++) {
           if (!((dirs >> k) & 1u)) continue;
-          long long nl = l;
-          if (k != DIR_SELF) {
-            int p[3] = {c[0], c[1], c[2]};
-            p[k >> 2] += dir_off(k);
-            nl = lin3(P.g, p[0], p[1], p[2]);
-          }
+          const long long nl = dir_lin(P.g, l, k);
           if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
         }
         __syncwarp();
@@ -280,12 +273,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
         wbase = __shfl_sync(0xffffffffu, wbase, 0) + (unsigned int)(incl - cntl);
         for (int k = 0; k <= DIR_SELF; k++) {
           if (!((keep >> k) & 1u)) continue;
-          long long nl = l;
-          if (k != DIR_SELF) {
-            int p[3] = {c[0], c[1], c[2]};
-            p[k >> 2] += dir_off(k);
-            nl = lin3(P.g, p[0], p[1], p[2]);
-          }
+          const long long nl = dir_lin(P.g, l, k);
           Lnext[wbase++] = list_entry((unsigned int)(gbase + nl), front);
         }
         {
@@ -347,18 +335,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
         PH_T(ts);
         // list the next round's nodes once each (per-node round stamps)
         const CoarseProblem& P = a.probs[prob];
-        const int c[3] = {(int)(l % P.g.n[0]), (int)((l / P.g.n[0]) % P.g.n[1]),
-                          (int)(l / ((long long)P.g.n[0] * P.g.n[1]))};
         const unsigned long long gbase = (unsigned long long)prob * N;
         unsigned keep = 0;
         for (int k = 0; k <= DIR_SELF; k++) {
           if (!((dirs >> k) & 1u)) continue;
-          long long nl = l;
-          if (k != DIR_SELF) {
-            int p[3] = {c[0], c[1], c[2]};
-            p[k >> 2] += dir_off(k);
-            nl = lin3(P.g, p[0], p[1], p[2]);
-          }
+          const long long nl = dir_lin(P.g, l, k);
           if (atomicExch(a.rs.stamp + gbase + nl, r + 1) != r + 1) keep |= 1u << k;
         }
         __syncwarp();
@@ -378,12 +359,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
         wbase = __shfl_sync(0xffffffffu, wbase, 0) + (unsigned int)(incl - cntl);
         for (int k = 0; k <= DIR_SELF; k++) {
           if (!((keep >> k) & 1u)) continue;
-          long long nl = l;
-          if (k != DIR_SELF) {
-            int p[3] = {c[0], c[1], c[2]};
-            p[k >> 2] += dir_off(k);
-            nl = lin3(P.g, p[0], p[1], p[2]);
-          }
+          const long long nl = dir_lin(P.g, l, k);
           Lnext[wbase++] = list_entry((unsigned int)(gbase + nl), front);
         }
         {
@@ -416,8 +392,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
     PH_ADD(4, tb);
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, o);
-  if (lane == 0 && evals) atomicAdd(a.node_evals, evals);
+  unsigned long long ev = evals;
+  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
+  if (lane == 0 && ev) atomicAdd(a.node_evals, ev);
 #ifdef EIK_PHASE
   for (int k = 7; k < 11; k++) atomicAdd(&eik_phase[k - 2], vk[k]);  // per lane
 #endif

@@ -12,9 +12,14 @@ namespace eik {
 #ifdef EIK_PHASE
 #define PL_T(v) const long long v = clock64()
 #define PL_ADD(k, t0) vk[k] += (unsigned long long)(clock64() - (t0))
+typedef unsigned long long VisitCount;  // tuning builds also sum clock cycles in the counters
 #else
 #define PL_T(v)
 #define PL_ADD(k, t0)
+// Per-lane counters of one solve (visits by outcome, rule evaluations): a lane takes at most
+// one entry per round and a launch has ~10^4 lanes or more, so its counts stay far below 2^32
+// (2^32 node-sources per launch x ~13 visits); 32 bits keep them out of a second register each.
+typedef unsigned int VisitCount;
 #endif
 
 // ------------------------------------------------------------------ node solve --
@@ -32,6 +37,24 @@ __device__ __forceinline__ void node_key(const CoarseProblem& P, long long l, do
 // Neighbour directions of a node: k = 4*axis + {0: -2, 1: -1, 2: +1, 3: +2}; bit 12 = itself.
 constexpr int DIR_SELF = 12;
 __device__ __forceinline__ int dir_off(int k) { return (k & 3) < 2 ? (k & 3) - 2 : (k & 3) - 1; }
+// Linear index of the node in direction k (or DIR_SELF) of node l, which the direction must
+// keep in the grid: the grid is column-major (lin3), so a step along an axis adds that axis's
+// stride. Arithmetic only: an array indexed by the loop's axis would live in local memory.
+// Grid coordinates of node l. A problem has fewer than 2^32 nodes (a launch numbers its
+// node-sources in 32 bits), so 32-bit division is exact and far cheaper than 64-bit.
+__device__ __forceinline__ void node_coords(const GridDesc& g, long long l, int* c) {
+  const unsigned ul = (unsigned)l, n0 = (unsigned)g.n[0], n1 = (unsigned)g.n[1];
+  const unsigned q = ul / n0;
+  c[0] = (int)(ul - q * n0);
+  c[1] = (int)(q % n1);
+  c[2] = (int)(q / n1);
+}
+__device__ __forceinline__ long long dir_lin(const GridDesc& g, long long l, int k) {
+  if (k == DIR_SELF) return l;
+  const int ax = k >> 2;
+  const long long st = ax == 0 ? 1LL : (ax == 1 ? (long long)g.n[0] : (long long)g.n[0] * g.n[1]);
+  return l + dir_off(k) * st;
+}
 
 // The round-solver state of problem P in global memory: node l at l (problem arrays) and at
 // gb + l (round-solver arrays, numbered over the problems of a launch).
@@ -54,33 +77,46 @@ struct GlobalNodes {
 };
 
 // The order rule on a neighbourhood with special keys (source points, non-causal
-// acceptances): the full keys of the immediate and distance-2 neighbours (arrays indexed
-// 2*axis + side; l < 0 where there is no such node). Kept out of line: it is rare, and its
-// key registers would otherwise weigh on every visit.
+// acceptances), from the full keys of the immediate and distance-2 neighbours. Kept out of
+// line because it is rare; its inputs and outputs go by value, so that no array of the visit
+// has its address taken (which would keep it in local memory on every visit).
+struct RuleIn {
+  long long l1[3][2], l2[3][2];  // neighbour indices, < 0 where there is no such node
+  double t1[3][2], t2[3][2];
+  uint8_t cd1[3][2], cd2[3][2];
+  double dh[3];
+  double slow;
+};
+struct RuleOut {
+  double v;
+  Key key;
+  int8_t cd[3];
+  bool neg;
+};
 template <int ND>
-__device__ __noinline__ double rule_full(const CoarseProblem& P, const long long* l1, const long long* l2,
-                                         const double* t1, const double* t2, const uint8_t* cd1, const uint8_t* cd2,
-                                         const double* dh, double slow, int8_t* cd, Key* nk, bool* neg) {
+__device__ __noinline__ RuleOut rule_full(const CoarseProblem& P, const RuleIn in) {
   Nbhd nb;
   nb_clear(nb);
-  for (int ax = 0; ax < 3; ax++) nb.dh[ax] = dh[ax];
-  nb.slow = slow;
+  for (int ax = 0; ax < 3; ax++) nb.dh[ax] = in.dh[ax];
+  nb.slow = in.slow;
   nb.c1u = P.c1u;
   nb.c2u = P.c2u;
   for (int ax = 0; ax < ND; ax++)
     for (int s = 0; s < 2; s++) {
-      const int k = 2 * ax + s;
-      if (l1[k] < 0) continue;
+      if (in.l1[ax][s] < 0) continue;
       double L;
       int d;
-      node_key(P, l1[k], t1[k], cd1[k], &L, &d);
-      nb_put1(nb, ax, s, t1[k], L, d);
-      if (l2[k] >= 0) {
-        node_key(P, l2[k], t2[k], cd2[k], &L, &d);
-        nb_put2(nb, ax, s, t2[k], L, d);
+      node_key(P, in.l1[ax][s], in.t1[ax][s], in.cd1[ax][s], &L, &d);
+      nb_put1(nb, ax, s, in.t1[ax][s], L, d);
+      if (in.l2[ax][s] >= 0) {
+        node_key(P, in.l2[ax][s], in.t2[ax][s], in.cd2[ax][s], &L, &d);
+        nb_put2(nb, ax, s, in.t2[ax][s], L, d);
       }
     }
-  return prefix_rule<ND>(nb, cd, nk, neg);
+  RuleOut o;
+  o.neg = false;
+  o.v = prefix_rule<ND>(nb, o.cd, &o.key, &o.neg);
+  return o;
 }
 
 // One listed node: gate, evaluate, write back. Returns the directions of the nodes to list
@@ -97,10 +133,11 @@ __device__ __noinline__ double rule_full(const CoarseProblem& P, const long long
 // can observe (see the notes at each stage).
 template <int ND, class M>
 __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem& P, long long l, double T, int r,
-                                                 double* front, unsigned long long* evals, unsigned long long* vk) {
+                                                 double* front, VisitCount* evals, VisitCount* vk) {
   PL_T(tq0);
   const GridDesc& g = P.g;
-  const int c[3] = {(int)(l % g.n[0]), (int)((l / g.n[0]) % g.n[1]), (int)(l / ((long long)g.n[0] * g.n[1]))};
+  int c[3];
+  node_coords(g, l, c);
   // The node's own state in one batch. Only this visit writes its t, code and key during
   // the round (a node is listed once per round), so their order of reading is free.
   const uint8_t dirty0 = m.dirty(l);
@@ -246,7 +283,28 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
     nb.c2u = P.c2u;
     nv = prefix_rule_plain<ND>(nb, cd, &nk, &neg);
   } else {
-    nv = rule_full<ND>(P, &l1[0][0], &l2[0][0], &t1[0][0], &t2[0][0], &cd1[0][0], &cd2[0][0], dh, slow, cd, &nk, &neg);
+    RuleIn in;
+#pragma unroll
+    for (int ax = 0; ax < 3; ax++) {
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const bool use = ax < ND;
+        in.l1[ax][s] = use ? l1[ax < ND ? ax : 0][s] : -1;
+        in.l2[ax][s] = use ? l2[ax < ND ? ax : 0][s] : -1;
+        in.t1[ax][s] = use ? t1[ax < ND ? ax : 0][s] : EIK_INF;
+        in.t2[ax][s] = use ? t2[ax < ND ? ax : 0][s] : EIK_INF;
+        in.cd1[ax][s] = use ? cd1[ax < ND ? ax : 0][s] : (uint8_t)0;
+        in.cd2[ax][s] = use ? cd2[ax < ND ? ax : 0][s] : (uint8_t)0;
+      }
+      in.dh[ax] = dh[ax];
+    }
+    in.slow = slow;
+    const RuleOut o = rule_full<ND>(P, in);
+    nv = o.v;
+    nk = o.key;
+    neg = o.neg;
+#pragma unroll
+    for (int a = 0; a < 3; a++) cd[a] = o.cd[a];
   }
   PL_ADD(9, tq2);
   (*evals)++;
