@@ -316,7 +316,6 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
     }
   }
   // counters: evaluations, visit outcomes, the largest round count
-#pragma unroll
   unsigned long long ev = evals;
   for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
   if (lane == 0 && ev) atomicAdd(a.node_evals, ev);

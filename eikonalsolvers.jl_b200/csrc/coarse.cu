@@ -391,7 +391,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
     if (!grid_barrier(a)) break;
     PH_ADD(4, tb);
   }
-#pragma unroll
   unsigned long long ev = evals;
   for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
   if (lane == 0 && ev) atomicAdd(a.node_evals, ev);

@@ -161,24 +161,27 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   // marks it dirty again (writers store the value, fence, then the flag)
   m.set_dirty(l, 0);
   m.fence();
-  // immediate neighbours (one batch with the slowness): potential = smallest traveltime
+  // immediate neighbours (one batch with the slowness): potential = smallest traveltime.
+  // Indices are 32-bit (a problem has fewer than 2^32 nodes) with a presence bit per
+  // neighbour (bit slot(ax, s)): half the registers of 64-bit indices with -1 for "none".
+  const unsigned ul = (unsigned)l;
+  const unsigned st1 = (unsigned)g.n[0], st2 = (unsigned)g.n[0] * (unsigned)g.n[1];
   double t1[ND][2];
-  long long l1[ND][2];
+  unsigned l1[ND][2];
+  unsigned in1 = 0u;
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
     for (int s = 0; s < 2; s++) {
       const int sh = s == 0 ? 1 : -1;
-      l1[ax][s] = -1;
-      if (c[ax] + sh < 0 || c[ax] + sh >= g.n[ax]) continue;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += sh;
-      l1[ax][s] = lin3(g, p[0], p[1], p[2]);
+      const unsigned st = ax == 0 ? 1u : (ax == 1 ? st1 : st2);
+      l1[ax][s] = s == 0 ? ul + st : ul - st;
+      if (c[ax] + sh >= 0 && c[ax] + sh < g.n[ax]) in1 |= 1u << slot(ax, s);
     }
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
-    for (int s = 0; s < 2; s++) t1[ax][s] = l1[ax][s] >= 0 ? m.t(l1[ax][s]) : EIK_INF;
+    for (int s = 0; s < 2; s++) t1[ax][s] = ((in1 >> slot(ax, s)) & 1u) ? m.t(l1[ax][s]) : EIK_INF;
   const double slow = __ldg(P.slow + l);
   double pot = EIK_INF;
 #pragma unroll
@@ -212,32 +215,32 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   // only together with the traveltime, in the neighbour's own visit.
   uint8_t cd1[ND][2], cd2[ND][2];
   double t2[ND][2];
-  long long l2[ND][2];
+  unsigned l2[ND][2];
+  unsigned ok2 = 0u;
+  // isonbord on the first neighbour, in every coordinate (eikutils.jl:129-162): the other
+  // coordinates are the node's own, the one along ax is one step out
 #pragma unroll
-  for (int ax = 0; ax < ND; ax++)
+  for (int ax = 0; ax < ND; ax++) {
+    bool side = true;
+#pragma unroll
+    for (int dd = 0; dd < ND; dd++)
+      if (dd != ax) side = side && c[dd] >= 1 && c[dd] <= g.n[dd] - 2;
 #pragma unroll
     for (int s = 0; s < 2; s++) {
       const int sh = s == 0 ? 1 : -1;
-      l2[ax][s] = -1;
-      if (l1[ax][s] < 0) continue;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += sh;
-      bool ok = true;  // isonbord on the first neighbour, in every coordinate (eikutils.jl:129-162)
-#pragma unroll
-      for (int dd = 0; dd < ND; dd++)
-        if (p[dd] < 1 || p[dd] > g.n[dd] - 2) ok = false;
-      if (ok) {
-        p[ax] += sh;
-        l2[ax][s] = lin3(g, p[0], p[1], p[2]);
-      }
+      const unsigned st = ax == 0 ? 1u : (ax == 1 ? st1 : st2);
+      l2[ax][s] = s == 0 ? l1[ax][s] + st : l1[ax][s] - st;
+      if (side && c[ax] + sh >= 1 && c[ax] + sh <= g.n[ax] - 2) ok2 |= 1u << slot(ax, s);
     }
+  }
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-      cd1[ax][s] = l1[ax][s] >= 0 ? m.code(l1[ax][s]) : (uint8_t)0;
-      t2[ax][s] = l2[ax][s] >= 0 ? m.t(l2[ax][s]) : EIK_INF;
-      cd2[ax][s] = l2[ax][s] >= 0 ? m.code(l2[ax][s]) : (uint8_t)0;
+      const bool h1 = (in1 >> slot(ax, s)) & 1u, h2 = (ok2 >> slot(ax, s)) & 1u;
+      cd1[ax][s] = h1 ? m.code(l1[ax][s]) : (uint8_t)0;
+      t2[ax][s] = h2 ? m.t(l2[ax][s]) : EIK_INF;
+      cd2[ax][s] = h2 ? m.code(l2[ax][s]) : (uint8_t)0;
     }
   // Without a special key among them (the common case) every key is the traveltime: the
   // rule runs on traveltimes alone (prefix_rule_plain), else on the full keys (rule_full).
@@ -245,10 +248,8 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
 #pragma unroll
   for (int ax = 0; ax < ND; ax++)
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
-      if (l1[ax][s] >= 0 && (cd1[ax][s] & CODE_SRC_BIT)) plain = false;
-      if (l2[ax][s] >= 0 && (cd2[ax][s] & CODE_SRC_BIT)) plain = false;
-    }
+    for (int s = 0; s < 2; s++)
+      if ((cd1[ax][s] | cd2[ax][s]) & CODE_SRC_BIT) plain = false;
   int8_t cd[3] = {0, 0, 0};
   Key nk;
   bool neg = false;
@@ -256,25 +257,14 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   double nv;
   if (plain) {
     NbhdT nb;
-    nb.in1 = nb.ok2 = 0u;
+    nb.in1 = in1;
+    nb.ok2 = ok2;  // within in1: a distance-2 node lies beyond an immediate one
 #pragma unroll
     for (int ax = 0; ax < 3; ax++)
 #pragma unroll
       for (int s = 0; s < 2; s++) {
-        nb.t1[ax][s] = EIK_INF;
-        nb.t2[ax][s] = EIK_INF;
-      }
-#pragma unroll
-    for (int ax = 0; ax < ND; ax++)
-#pragma unroll
-      for (int s = 0; s < 2; s++) {
-        if (l1[ax][s] < 0) continue;
-        nb.t1[ax][s] = t1[ax][s];
-        nb.in1 |= 1u << slot(ax, s);
-        if (l2[ax][s] >= 0) {
-          nb.t2[ax][s] = t2[ax][s];
-          nb.ok2 |= 1u << slot(ax, s);
-        }
+        nb.t1[ax][s] = ax < ND ? t1[ax < ND ? ax : 0][s] : EIK_INF;  // EIK_INF where absent
+        nb.t2[ax][s] = ax < ND ? t2[ax < ND ? ax : 0][s] : EIK_INF;
       }
 #pragma unroll
     for (int ax = 0; ax < 3; ax++) nb.dh[ax] = dh[ax];
@@ -289,8 +279,9 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
 #pragma unroll
       for (int s = 0; s < 2; s++) {
         const bool use = ax < ND;
-        in.l1[ax][s] = use ? l1[ax < ND ? ax : 0][s] : -1;
-        in.l2[ax][s] = use ? l2[ax < ND ? ax : 0][s] : -1;
+        const bool h1 = use && ((in1 >> slot(ax, s)) & 1u), h2 = use && ((ok2 >> slot(ax, s)) & 1u);
+        in.l1[ax][s] = h1 ? (long long)l1[ax < ND ? ax : 0][s] : -1;
+        in.l2[ax][s] = h2 ? (long long)l2[ax < ND ? ax : 0][s] : -1;
         in.t1[ax][s] = use ? t1[ax < ND ? ax : 0][s] : EIK_INF;
         in.t2[ax][s] = use ? t2[ax < ND ? ax : 0][s] : EIK_INF;
         in.cd1[ax][s] = use ? cd1[ax < ND ? ax : 0][s] : (uint8_t)0;
@@ -349,28 +340,28 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   unsigned dirs = 0;
 #pragma unroll
   for (int ax = 0; ax < ND; ax++) {
-    long long lj[4];
+    const unsigned st = ax == 0 ? 1u : (ax == 1 ? st1 : st2);
+    unsigned lj[4];
+    unsigned hj = 0u;  // bit j: the node exists
     double tj[4];
     uint8_t cj[4];
     int32_t sj[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) {
       const int off = dir_off(j);
-      lj[j] = -1;
-      if (c[ax] + off < 0 || c[ax] + off >= g.n[ax]) continue;
-      int p[3] = {c[0], c[1], c[2]};
-      p[ax] += off;
-      lj[j] = lin3(g, p[0], p[1], p[2]);
+      lj[j] = off < 0 ? ul - (unsigned)(-off) * st : ul + (unsigned)off * st;
+      if (c[ax] + off >= 0 && c[ax] + off < g.n[ax]) hj |= 1u << j;
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      tj[j] = lj[j] >= 0 ? m.t(lj[j]) : EIK_INF;
-      cj[j] = lj[j] >= 0 ? m.code(lj[j]) : (uint8_t)0;
-      sj[j] = lj[j] >= 0 ? m.stamp(lj[j]) : 0;
+      const bool h = (hj >> j) & 1u;
+      tj[j] = h ? m.t(lj[j]) : EIK_INF;
+      cj[j] = h ? m.code(lj[j]) : (uint8_t)0;
+      sj[j] = h ? m.stamp(lj[j]) : 0;
     }
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      if (lj[j] < 0) continue;
+      if (!((hj >> j) & 1u)) continue;
       // j = 0 (-2) reads this node through j = 1 (-1), j = 3 (+2) through j = 2 (+1)
       if (j == 0 && !(tj[1] < EIK_INF)) continue;
       if (j == 3 && !(tj[2] < EIK_INF)) continue;
