@@ -47,6 +47,7 @@ struct ClusterCtl {
   unsigned int cnt[3];
   unsigned int grab[3];
   unsigned long long nm[3];  // smallest pending front listed for a round (double bits)
+  unsigned long long visits[CL_THREADS / 32][8];  // per-warp visit counts by outcome (this CTA's)
 };
 
 // The round-solver state of one problem in a cluster's distributed shared memory.
@@ -182,11 +183,12 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
   }
   cl.sync();
 
-  VisitCount evals = 0;
+  unsigned long long* wvis = ctl.visits[threadIdx.x >> 5];
+  clear_visits(wvis, lane);
 #ifdef EIK_PHASE
-  VisitCount vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles of the node visit
+  VisitCount vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // lane cycles of the node visit at 7..10
 #else
-  VisitCount vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
+  VisitCount* vk = nullptr;
 #endif
   double Tprev = -EIK_INF;
   int r = 0;
@@ -234,7 +236,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
       base = __shfl_sync(0xffffffffu, base, 0);
       if (base >= n) break;
       const unsigned int idx = base + lane;
-      unsigned dirs = 0;
+      unsigned dirs = visit_code(VISIT_NONE);
       double front = EIK_INF;
       long long l = 0;
       if (idx < n) {
@@ -245,13 +247,13 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
         if (ef > T && ef < EIK_INF && !dq) {
           // still waiting and nothing it reads has changed: its front stands
           front = ef;
-          dirs = 1u << DIR_SELF;
-          vk[0]++;
+          dirs = (1u << DIR_SELF) | visit_code(VISIT_STANDS);
         } else {
-          dirs = process_node<ND>(m, P, l, T, r, &front, &evals, vk);
+          dirs = process_node<ND>(m, P, l, T, r, &front, vk);
         }
       }
       __syncwarp();
+      count_visits(wvis, dirs, lane);
       CPH_ADD(1, tp0);
       CPH_T(tp1);
       // list the next round's nodes once each (round stamps) with their owners; the stamp
@@ -316,14 +318,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1)
     }
   }
   // counters: evaluations, visit outcomes, the largest round count
-  unsigned long long ev = evals;
-  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
-  if (lane == 0 && ev) atomicAdd(a.node_evals, ev);
-  for (int k = 0; k < 7; k++) {
-    unsigned long long v = vk[k];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0 && v) atomicAdd(a.rs.visits + k, v);
-  }
+  flush_visits(wvis, a.rs.visits, a.node_evals, lane);
   if (rank == 0 && threadIdx.x == 0) {
     atomicMax(a.rs.rounds, r);
     if (r >= a.rs.max_rounds) atomicOr(a.err, ERRB_NOT_CONVERGED);

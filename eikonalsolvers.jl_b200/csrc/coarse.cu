@@ -112,16 +112,19 @@ __global__ void seed_kernel(SolveArgs a, const int32_t* seed_lin, const double* 
 }
 
 #ifdef EIK_PHASE
-// tuning builds only: clock cycles per phase summed over warps (lane 0)
-__device__ unsigned long long eik_phase[9];
+// tuning builds only: clock cycles per phase summed over warps (lane 0); 9..11: cycles of
+// the entry loads of a queue fill, and the counts of fill and evaluation steps
+__device__ unsigned long long eik_phase[12];
 extern "C" int eik_phase_read(unsigned long long* out) {
-  return (int)cudaMemcpyFromSymbol(out, eik_phase, sizeof(unsigned long long) * 9);
+  return (int)cudaMemcpyFromSymbol(out, eik_phase, sizeof(unsigned long long) * 12);
 }
 #define PH_T(v) const long long v = clock64()
 #define PH_ADD(k, t0) if ((threadIdx.x & 31) == 0) atomicAdd(&eik_phase[k], (unsigned long long)(clock64() - (t0)))
+#define PH_CNT(k) if ((threadIdx.x & 31) == 0) atomicAdd(&eik_phase[k], 1ull)
 #else
 #define PH_T(v)
 #define PH_ADD(k, t0)
+#define PH_CNT(k)
 #endif
 __device__ __forceinline__ double warp_min(double v) {
 #pragma unroll
@@ -157,12 +160,15 @@ template <int ND, bool QUEUE, int MB>
 __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveArgs a) {
   const int lane = threadIdx.x & 31;
   __shared__ unsigned long long wq[SOLVE_THREADS / 32][QUEUE ? 64 : 1];  // per-warp queue of entries to evaluate
+  __shared__ unsigned long long wv[SOLVE_THREADS / 32][8];  // per-warp visit counts by outcome
   const unsigned long long N = a.rs.stride;  // node id = problem * stride + node
-  VisitCount evals = 0;
+  const unsigned N32 = (unsigned)N;            // node ids are 32-bit: so is the stride
+  unsigned long long* wvis = wv[threadIdx.x >> 5];
+  clear_visits(wvis, lane);
 #ifdef EIK_PHASE
-  VisitCount vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // + lane cycles: gates, node path, rule, relist filter
+  VisitCount vk[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // lane cycles at 7..10: gates, node path, rule, relist filter
 #else
-  VisitCount vk[7] = {0, 0, 0, 0, 0, 0, 0};  // visit outcomes, see eik_stats.fwd_visits
+  VisitCount* vk = nullptr;
 #endif
   int r = 0;
   for (; r < a.rs.max_rounds; r++) {
@@ -187,7 +193,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
       int qn = 0;  // queued entries (warp-uniform)
       bool more = true;
       while (more || qn > 0) {
-        unsigned dirs = 0;
+        unsigned dirs = visit_code(VISIT_NONE);
         double front = EIK_INF;
         int prob = 0;
         long long l = 0;
@@ -201,6 +207,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
             more = false;
             continue;
           }
+          PH_T(tl);
+          PH_CNT(10);
           const unsigned int idx = base + lane;
           bool queue = false;
           unsigned long long e = 0;
@@ -208,7 +216,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
             e = __ldcg(L + idx);
             const unsigned int gid = (unsigned int)(e >> 32);
             const double ef = (double)__uint_as_float((unsigned int)e);
-            prob = (int)(gid / N);
+            prob = (int)(gid / N32);
             l = (long long)(gid - (unsigned long long)prob * N);
             // threshold inputs and the dirty flag in one batch
             const double tp = __ldcg(thr_prev + prob);
@@ -218,8 +226,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
             const double T = fmax(tp, __longlong_as_double((long long)nmv) + del);
             if (ef > T && ef < EIK_INF && !dq) {
               front = ef;
-              dirs = 1u << DIR_SELF;
-              vk[0]++;
+              dirs = (1u << DIR_SELF) | visit_code(VISIT_STANDS);
             } else {
               queue = true;
             }
@@ -228,24 +235,27 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
           if (queue) q[qn + __popc(qm & ((1u << lane) - 1u))] = e;
           qn += __popc(qm);
           __syncwarp();
+          PH_ADD(9, tl);
         } else {
           PH_T(tp);
+          PH_CNT(11);
           const int k = qn < 32 ? qn : 32;
           if (lane < k) {
             const unsigned long long e = q[qn - k + lane];
             const unsigned int gid = (unsigned int)(e >> 32);
-            prob = (int)(gid / N);
+            prob = (int)(gid / N32);
             l = (long long)(gid - (unsigned long long)prob * N);
             const CoarseProblem& P = a.probs[prob];
             const double T = fmax(__ldcg(thr_prev + prob), __longlong_as_double((long long)ld_volatile(nm + prob)) + P.delta);
             const unsigned long long gb = (unsigned long long)prob * N;
-            dirs = (ND == 3) ? process_node<3>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk)
-                             : process_node<2>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk);
+            dirs = (ND == 3) ? process_node<3>(GlobalNodes{a, P, gb}, P, l, T, r, &front, vk)
+                             : process_node<2>(GlobalNodes{a, P, gb}, P, l, T, r, &front, vk);
           }
           qn -= k;
           __syncwarp();
           PH_ADD(1, tp);
         }
+        count_visits(wvis, dirs, lane);
         PH_T(ts);
         // list the next round's nodes once each (per-node round stamps)
         const CoarseProblem& P = a.probs[prob];
@@ -301,7 +311,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
         if (base >= n) break;
         PH_T(tp);
         const unsigned int idx = base + lane;
-        unsigned dirs = 0;
+        unsigned dirs = visit_code(VISIT_NONE);
         double front = EIK_INF;
         int prob = 0;
         long long l = 0;
@@ -309,7 +319,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
           const unsigned long long e = __ldcg(L + idx);
           const unsigned int gid = (unsigned int)(e >> 32);
           const double ef = (double)__uint_as_float((unsigned int)e);
-          prob = (int)(gid / N);
+          prob = (int)(gid / N32);
           l = (long long)(gid - (unsigned long long)prob * N);
           const CoarseProblem& P = a.probs[prob];
           // window of one round width above the smallest pending front, never moving back
@@ -323,15 +333,15 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
           if (ef > T && ef < EIK_INF && !dq) {
             // still waiting and nothing it reads has changed: its front stands
             front = ef;
-            dirs = 1u << DIR_SELF;
-            vk[0]++;
+            dirs = (1u << DIR_SELF) | visit_code(VISIT_STANDS);
           } else {
-            dirs = (ND == 3) ? process_node<3>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk)
-                             : process_node<2>(GlobalNodes{a, P, gb}, P, l, T, r, &front, &evals, vk);
+            dirs = (ND == 3) ? process_node<3>(GlobalNodes{a, P, gb}, P, l, T, r, &front, vk)
+                             : process_node<2>(GlobalNodes{a, P, gb}, P, l, T, r, &front, vk);
           }
         }
         __syncwarp();
         PH_ADD(1, tp);
+        count_visits(wvis, dirs, lane);
         PH_T(ts);
         // list the next round's nodes once each (per-node round stamps)
         const CoarseProblem& P = a.probs[prob];
@@ -391,19 +401,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS, MB) coarse_rounds_kernel(SolveA
     if (!grid_barrier(a)) break;
     PH_ADD(4, tb);
   }
-  unsigned long long ev = evals;
-  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
-  if (lane == 0 && ev) atomicAdd(a.node_evals, ev);
+  flush_visits(wvis, a.rs.visits, a.node_evals, lane);
 #ifdef EIK_PHASE
   for (int k = 7; k < 11; k++) atomicAdd(&eik_phase[k - 2], vk[k]);  // per lane
 #endif
-#pragma unroll
-  for (int k = 0; k < 7; k++) {
-    unsigned long long v = vk[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0 && v) atomicAdd(a.rs.visits + k, v);
-  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *a.rs.rounds = r;
     if (r >= a.rs.max_rounds) {

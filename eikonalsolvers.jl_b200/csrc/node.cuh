@@ -10,17 +10,58 @@
 namespace eik {
 
 #ifdef EIK_PHASE
+// tuning builds sum the clock cycles of the visit's stages per lane (vk[7..10])
 #define PL_T(v) const long long v = clock64()
 #define PL_ADD(k, t0) vk[k] += (unsigned long long)(clock64() - (t0))
-typedef unsigned long long VisitCount;  // tuning builds also sum clock cycles in the counters
 #else
 #define PL_T(v)
 #define PL_ADD(k, t0)
-// Per-lane counters of one solve (visits by outcome, rule evaluations): a lane takes at most
-// one entry per round and a launch has ~10^4 lanes or more, so its counts stay far below 2^32
-// (2^32 node-sources per launch x ~13 visits); 32 bits keep them out of a second register each.
-typedef unsigned int VisitCount;
 #endif
+typedef unsigned long long VisitCount;
+
+// Visit outcomes, in the order of eik_stats.fwd_visits. process_node returns the outcome in
+// bits VISIT_SHIFT.. of its result, above the direction bits; VISIT_NONE marks a lane that
+// visited nothing in a step.
+constexpr int VISIT_SHIFT = 16;
+enum : unsigned {
+  VISIT_STANDS = 0,  // value cached above the front, nothing it reads changed
+  VISIT_SOURCE,      // source point (fixed)
+  VISIT_UNREACHED,   // no neighbour reached yet
+  VISIT_BOUND,       // lower bound above the front
+  VISIT_WAIT,        // evaluated, above the front
+  VISIT_SAME,        // evaluated, value and key unchanged
+  VISIT_CHANGED,     // evaluated and accepted
+  VISIT_NONE
+};
+__device__ __forceinline__ unsigned visit_code(unsigned v) { return v << VISIT_SHIFT; }
+
+// Adds one step's visit outcomes of a (converged) warp to the warp's counters in shared
+// memory, w[0..6]: three ballots split the lanes by outcome. Counting in shared memory keeps
+// seven per-lane counters out of the registers of the visit.
+__device__ __forceinline__ void count_visits(unsigned long long* w, unsigned res, int lane) {
+  const unsigned oc = (res >> VISIT_SHIFT) & 7u;
+  const unsigned b0 = __ballot_sync(0xffffffffu, oc & 1u), b1 = __ballot_sync(0xffffffffu, oc & 2u),
+                 b2 = __ballot_sync(0xffffffffu, oc & 4u);
+  if (lane < 7) {
+    const unsigned mk = ((lane & 1) ? b0 : ~b0) & ((lane & 2) ? b1 : ~b1) & ((lane & 4) ? b2 : ~b2);
+    w[lane] += (unsigned long long)__popc(mk);
+  }
+}
+__device__ __forceinline__ void clear_visits(unsigned long long* w, int lane) {
+  if (lane < 8) w[lane] = 0;
+  __syncwarp();
+}
+// Adds a warp's counters to the solve's: visits by outcome, and the evaluations of the order
+// rule (the outcomes that follow one: wait, same, changed).
+__device__ __forceinline__ void flush_visits(const unsigned long long* w, unsigned long long* visits,
+                                             unsigned long long* evals, int lane) {
+  __syncwarp();
+  if (lane < 7 && w[lane]) atomicAdd(visits + lane, w[lane]);
+  if (lane == 0) {
+    const unsigned long long ev = w[VISIT_WAIT] + w[VISIT_SAME] + w[VISIT_CHANGED];
+    if (ev) atomicAdd(evals, ev);
+  }
+}
 
 // ------------------------------------------------------------------ node solve --
 // Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise.
@@ -120,7 +161,8 @@ __device__ __noinline__ RuleOut rule_full(const CoarseProblem& P, const RuleIn i
 }
 
 // One listed node: gate, evaluate, write back. Returns the directions of the nodes to list
-// for the next round (bit DIR_SELF: this node again) and, in *front, the traveltime that
+// for the next round (bit DIR_SELF: this node again) with the visit's outcome
+// (visit_code) above them and, in *front, the traveltime that
 // bounds their next evaluation from below. M holds the problem's round-solver state (the
 // node's traveltime, code, cached front, dirty flag and round stamp): global memory
 // (GlobalNodes) or the distributed shared memory of a thread-block cluster; key levels and
@@ -133,7 +175,7 @@ __device__ __noinline__ RuleOut rule_full(const CoarseProblem& P, const RuleIn i
 // can observe (see the notes at each stage).
 template <int ND, class M>
 __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem& P, long long l, double T, int r,
-                                                 double* front, VisitCount* evals, VisitCount* vk) {
+                                                 double* front, VisitCount* vk) {
   PL_T(tq0);
   const GridDesc& g = P.g;
   int c[3];
@@ -147,15 +189,13 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   // last evaluated value, still valid while nothing the node reads has changed
   if (!dirty0 && tv > T && tv < EIK_INF) {
     *front = tv;
-    vk[0]++;
-    return 1u << DIR_SELF;
+    return (1u << DIR_SELF) | visit_code(VISIT_STANDS);
   }
   double Lold;
   int dold;
   node_key(P, l, told, cb, &Lold, &dold);
   if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) {  // source points are fixed
-    vk[1]++;
-    return 0;
+    return visit_code(VISIT_SOURCE);
   }
   // from here the node reads its neighbours' current values: a change after this point
   // marks it dirty again (writers store the value, fence, then the flag)
@@ -190,8 +230,7 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
     for (int s = 0; s < 2; s++) pot = fmin(pot, t1[ax][s]);
   if (!(pot < EIK_INF)) {  // nothing reached around it yet
     m.set_tent(l, EIK_INF);
-    vk[2]++;
-    return 0;
+    return visit_code(VISIT_UNREACHED);
   }
   PL_ADD(7, tq0);
   PL_T(tq1);
@@ -207,8 +246,7 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   if (lb > T) {
     m.set_tent(l, lb);  // stands, like an evaluated value, while the node stays clean
     *front = lb;
-    vk[3]++;
-    return 1u << DIR_SELF;
+    return (1u << DIR_SELF) | visit_code(VISIT_BOUND);
   }
   // Codes of the immediate neighbours and the distance-2 nodes with their codes, one batch.
   // A neighbour's key is read after its traveltime here as in any order: the key changes
@@ -298,7 +336,6 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
     for (int a = 0; a < 3; a++) cd[a] = o.cd[a];
   }
   PL_ADD(9, tq2);
-  (*evals)++;
   const uint8_t nc = pack_codes(cd, ND);
   const bool same_t = (nv == told) || (isinf(nv) && isinf(told));
   const bool tkchange = !(same_t && key_eq(nk, Key{Lold, dold, told}));
@@ -307,13 +344,11 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   m.set_tent(l, nv);
   if (!tkchange) {
     if (ncb != cb) m.set_code(l, ncb);
-    vk[5]++;
-    return 0;
+    return visit_code(VISIT_SAME);
   }
   if (nv > T) {  // not final yet: keep the old value and come back when the front is there
     *front = nv;
-    vk[4]++;
-    return 1u << DIR_SELF;
+    return (1u << DIR_SELF) | visit_code(VISIT_WAIT);
   }
   m.set_t(l, nv);
   m.set_code(l, ncb);
@@ -379,8 +414,7 @@ __device__ __forceinline__ unsigned process_node(const M& m, const CoarseProblem
   *front = nv + P.incmin;  // no node reading this one can get a smaller value from it
   PL_ADD(10, tq3);
   PL_ADD(8, tq1);
-  vk[6]++;
-  return dirs;
+  return dirs | visit_code(VISIT_CHANGED);
 }
 
 }  // namespace eik

@@ -127,3 +127,17 @@ def test_many_sources_batched_at_128cubed_match_the_oracle(ctx):
                                   extraparams=ExtraParams())
         assert int((tt[s] != ott[0]).sum()) == 0, s
         assert np.array_equal(picks[s], op[0])
+
+
+@pytest.mark.parametrize("which", ["2d_cluster", "3d_global"])
+def test_visit_counts_add_up(ctx, which):
+    """Without the refined start-up every list entry of the coarse solve is visited once, with
+    one outcome: the outcome counts sum to the list entries, and the three outcomes that
+    follow an evaluation of the order rule sum to the evaluations."""
+    w = CF.cfg2(scale=0.125, nsrc=3) if which == "2d_cluster" else CF.cfg3(scale=0.125, nsrc=3, nrec_side=3)
+    _run(ctx, w.vel, w.grd, w.coordsrc, w.coordrec, ExtraParams(refinearoundsrc=False))
+    st = ctx.last_stats
+    vis = [int(v) for v in st.fwd_visits]
+    assert st.node_evals > 0 and st.retries == 0
+    assert sum(vis) == int(st.tile_activations), vis
+    assert vis[4] + vis[5] + vis[6] == int(st.node_evals), vis
