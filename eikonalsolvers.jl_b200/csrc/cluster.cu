@@ -38,7 +38,10 @@ namespace cg = cooperative_groups;
 
 namespace eik {
 
-constexpr int CL_THREADS = 512;         // threads per CTA
+// Threads per CTA. A round's front gives each CTA a few warps' worth of entries, and the
+// round lasts as long as the slowest warp's visit: 256 threads leave the visit 180 registers
+// a thread and no spill, which shortens that chain more than 16 warps per CTA would help.
+constexpr int CL_THREADS = 256;
 constexpr int CL_MAX_LGC = 4;           // clusters of up to 16 CTAs
 constexpr int CL_BYTES_PER_NODE = 38;   // t, cached front, two list entries (8 B each), stamp (4), code, dirty
 
