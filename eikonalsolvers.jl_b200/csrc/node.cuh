@@ -17,7 +17,7 @@ namespace eik {
 #define PL_T(v)
 #define PL_ADD(k, t0)
 #endif
-typedef unsigned long long VisitCount;
+typedef unsigned long long VisitCount;  // the per-lane cycle sums (vk) of tuning builds
 
 // Visit outcomes, in the order of eik_stats.fwd_visits. process_node returns the outcome in
 // bits VISIT_SHIFT.. of its result, above the direction bits; VISIT_NONE marks a lane that
