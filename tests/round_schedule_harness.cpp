@@ -1,0 +1,422 @@
+// Host emulation of the forward round solver's schedule (test harness, not product code).
+//
+// Restates, one visit at a time, what coarse_rounds_kernel does to a Cartesian grid: worklist
+// rounds under the threshold T(r) = max(T(r-1), smallest pending front + delta), the node
+// visit of node.cuh (cached front, lower-bound gate, the order rule of stencil.cuh on
+// traveltimes alone or on full keys, write-back, relist filter) and the per-round stamps.
+// The order rule itself is the product's (stencil.cuh, compiled for the host). Visits within
+// a round run in list order (mode 0), in a seeded random order (mode 1), or in a random order
+// with waiting nodes parked by front instead of listed again every round (mode 2: a node
+// whose front still stands is taken out of the lists and comes back in the first round whose
+// threshold reaches its front, unless a neighbour's change lists it earlier).
+//
+// Usage: round_schedule_harness in.bin out.bin
+//   in:  int32 nd, n0, n1, n2; double h, gate; int32 mode; uint64 seed; int64 nseed;
+//        N doubles slowness (1/v, as the product computes it); nseed int64 node indices;
+//        nseed doubles traveltimes of the fixed source points.
+//   out: N doubles traveltime; int64 rounds, list entries, rule evaluations, visits by
+//        outcome (7: stands, source, unreached, bound, wait, same, changed), parked nodes
+//        taken back.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <algorithm>
+#include <cstring>
+#include <queue>
+#include <tuple>
+#include <random>
+#include <vector>
+
+#include "stencil.cuh"
+
+using namespace eik;
+
+namespace {
+
+struct Solver {
+  int nd;
+  int n[3];
+  double h;
+  long long N;
+  std::vector<double> slow, t, tent, kL;
+  std::vector<uint8_t> code, kd, dirty;
+  std::vector<int> stamp;
+  double delta, incmin, c1u, c2u;
+  long long evals = 0, visits[7] = {0, 0, 0, 0, 0, 0, 0};
+
+  long long lin(const int* c) const { return c[0] + (long long)n[0] * (c[1] + (long long)n[1] * c[2]); }
+  void coords(long long l, int* c) const {
+    c[0] = (int)(l % n[0]);
+    c[1] = (int)((l / n[0]) % n[1]);
+    c[2] = (int)(l / ((long long)n[0] * n[1]));
+  }
+  void key(long long l, double tv, uint8_t cb, double* L, int* d) const {
+    if (cb & CODE_SRC_BIT) {
+      *L = kL[l];
+      *d = kd[l];
+    } else {
+      *L = tv;
+      *d = 0;
+    }
+  }
+};
+
+// Float of the list entry: the front rounded down (the kernel's __double2float_rd).
+double entry_front(double f) {
+  if (!(f < EIK_INF)) return EIK_INF;
+  float g = (float)f;
+  if ((double)g > f) g = std::nextafterf(g, -INFINITY);
+  return (double)g;
+}
+
+enum { V_STANDS, V_SOURCE, V_UNREACHED, V_BOUND, V_WAIT, V_SAME, V_CHANGED };
+
+// One visit of node l in round r under threshold T (node.cuh, process_node). Returns the
+// directions to list (bit 4*ax+j for j = -2,-1,+1,+2; bit 12 itself) and the outcome.
+template <int ND>
+unsigned visit(Solver& S, long long l, double T, int r, double* front, int* outcome) {
+  int c[3];
+  S.coords(l, c);
+  const uint8_t dirty0 = S.dirty[l];
+  const double tv = S.tent[l];
+  const uint8_t cb = S.code[l];
+  const double told = S.t[l];
+  if (!dirty0 && tv > T && tv < EIK_INF) {
+    *front = tv;
+    *outcome = V_STANDS;
+    return 1u << 12;
+  }
+  double Lold;
+  int dold;
+  S.key(l, told, cb, &Lold, &dold);
+  if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) {
+    *outcome = V_SOURCE;
+    return 0;
+  }
+  S.dirty[l] = 0;
+  long long l1[3][2], l2[3][2];
+  double t1[3][2], t2[3][2];
+  uint8_t cd1[3][2], cd2[3][2];
+  double pot = EIK_INF;
+  for (int ax = 0; ax < ND; ax++)
+    for (int s = 0; s < 2; s++) {
+      const int sh = s == 0 ? 1 : -1;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      l1[ax][s] = (p[ax] < 0 || p[ax] >= S.n[ax]) ? -1 : S.lin(p);
+      t1[ax][s] = l1[ax][s] >= 0 ? S.t[l1[ax][s]] : EIK_INF;
+      pot = std::fmin(pot, t1[ax][s]);
+    }
+  if (!(pot < EIK_INF)) {
+    S.tent[l] = EIK_INF;
+    *outcome = V_UNREACHED;
+    return 0;
+  }
+  const double slow = S.slow[l];
+  const double hmin = S.h;
+  const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
+  if (lb > T) {
+    S.tent[l] = lb;
+    *front = lb;
+    *outcome = V_BOUND;
+    return 1u << 12;
+  }
+  bool plain = true;
+  for (int ax = 0; ax < ND; ax++)
+    for (int s = 0; s < 2; s++) {
+      const int sh = s == 0 ? 1 : -1;
+      l2[ax][s] = -1;
+      cd1[ax][s] = cd2[ax][s] = 0;
+      t2[ax][s] = EIK_INF;
+      if (l1[ax][s] < 0) continue;
+      cd1[ax][s] = S.code[l1[ax][s]];
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += sh;
+      bool ok = true;  // isonbord on the first neighbour
+      for (int dd = 0; dd < ND; dd++)
+        if (p[dd] < 1 || p[dd] > S.n[dd] - 2) ok = false;
+      if (ok) {
+        p[ax] += sh;
+        l2[ax][s] = S.lin(p);
+        t2[ax][s] = S.t[l2[ax][s]];
+        cd2[ax][s] = S.code[l2[ax][s]];
+      }
+      if ((cd1[ax][s] | cd2[ax][s]) & CODE_SRC_BIT) plain = false;
+    }
+  int8_t cd[3] = {0, 0, 0};
+  Key nk;
+  bool neg = false;
+  double nv;
+  if (plain) {
+    NbhdT nb;
+    nb.in1 = nb.ok2 = 0u;
+    for (int ax = 0; ax < 3; ax++)
+      for (int s = 0; s < 2; s++) {
+        nb.t1[ax][s] = EIK_INF;
+        nb.t2[ax][s] = EIK_INF;
+      }
+    for (int ax = 0; ax < ND; ax++)
+      for (int s = 0; s < 2; s++) {
+        if (l1[ax][s] < 0) continue;
+        nb.t1[ax][s] = t1[ax][s];
+        nb.in1 |= 1u << slot(ax, s);
+        if (l2[ax][s] >= 0) {
+          nb.t2[ax][s] = t2[ax][s];
+          nb.ok2 |= 1u << slot(ax, s);
+        }
+      }
+    for (int ax = 0; ax < 3; ax++) nb.dh[ax] = S.h;
+    nb.slow = slow;
+    nb.c1u = S.c1u;
+    nb.c2u = S.c2u;
+    nv = prefix_rule_plain<ND>(nb, cd, &nk, &neg);
+  } else {
+    Nbhd nb;
+    nb_clear(nb);
+    for (int ax = 0; ax < 3; ax++) nb.dh[ax] = S.h;
+    nb.slow = slow;
+    nb.c1u = S.c1u;
+    nb.c2u = S.c2u;
+    for (int ax = 0; ax < ND; ax++)
+      for (int s = 0; s < 2; s++) {
+        if (l1[ax][s] < 0) continue;
+        double L;
+        int d;
+        S.key(l1[ax][s], t1[ax][s], cd1[ax][s], &L, &d);
+        nb_put1(nb, ax, s, t1[ax][s], L, d);
+        if (l2[ax][s] >= 0) {
+          S.key(l2[ax][s], t2[ax][s], cd2[ax][s], &L, &d);
+          nb_put2(nb, ax, s, t2[ax][s], L, d);
+        }
+      }
+    nv = prefix_rule<ND>(nb, cd, &nk, &neg);
+  }
+  S.evals++;
+  const uint8_t nc = pack_codes(cd, ND);
+  const bool same_t = (nv == told) || (std::isinf(nv) && std::isinf(told));
+  const bool tkchange = !(same_t && key_eq(nk, Key{Lold, dold, told}));
+  const bool special = !(nk.L == nv && nk.d == 0);
+  const uint8_t ncb = (uint8_t)(nc | (special ? CODE_SRC_BIT : 0));
+  S.tent[l] = nv;
+  if (!tkchange) {
+    if (ncb != cb) S.code[l] = ncb;
+    *outcome = V_SAME;
+    return 0;
+  }
+  if (nv > T) {
+    *front = nv;
+    *outcome = V_WAIT;
+    return 1u << 12;
+  }
+  S.t[l] = nv;
+  S.code[l] = ncb;
+  if (special) {
+    S.kL[l] = nk.L;
+    S.kd[l] = (uint8_t)nk.d;
+  }
+  // relist filter
+  const Key kold = Key{Lold, dold, told};
+  unsigned dirs = 0;
+  for (int ax = 0; ax < ND; ax++) {
+    long long lj[4];
+    double tj[4];
+    for (int j = 0; j < 4; j++) {
+      const int off = j < 2 ? j - 2 : j - 1;
+      int p[3] = {c[0], c[1], c[2]};
+      p[ax] += off;
+      lj[j] = (p[ax] < 0 || p[ax] >= S.n[ax]) ? -1 : S.lin(p);
+      tj[j] = lj[j] >= 0 ? S.t[lj[j]] : EIK_INF;
+    }
+    for (int j = 0; j < 4; j++) {
+      if (lj[j] < 0) continue;
+      if (j == 0 && !(tj[1] < EIK_INF)) continue;
+      if (j == 3 && !(tj[2] < EIK_INF)) continue;
+      if (S.stamp[lj[j]] < r) {
+        double Lj;
+        int dj;
+        S.key(lj[j], tj[j], S.code[lj[j]], &Lj, &dj);
+        const Key kj = Key{Lj, dj, tj[j]};
+        if (key_le(kj, kold) && key_le(kj, nk)) continue;
+      }
+      S.dirty[lj[j]] = 1;
+      dirs |= 1u << (4 * ax + j);
+    }
+  }
+  *front = nv + S.incmin;
+  *outcome = V_CHANGED;
+  return dirs;
+}
+
+long long dir_node(const Solver& S, long long l, int k) {
+  if (k == 12) return l;
+  const int ax = k >> 2, j = k & 3;
+  const int off = j < 2 ? j - 2 : j - 1;
+  const long long st = ax == 0 ? 1 : (ax == 1 ? S.n[0] : (long long)S.n[0] * S.n[1]);
+  return l + off * st;
+}
+
+struct Entry {
+  long long l;
+  double f;  // front as stored in the list (rounded down to float)
+};
+
+template <int ND>
+void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<double>& seedtt, int mode,
+           unsigned long long seed, long long* rounds_out, long long* entries_out, long long* unparked_out) {
+  std::mt19937_64 rng(seed);
+  std::vector<Entry> cur, next;
+  double nm_next = EIK_INF, thr = -EIK_INF;
+  auto list = [&](int r, long long l, double f, std::vector<Entry>& L) {
+    if (S.stamp[l] != r) {
+      S.stamp[l] = r;
+      L.push_back(Entry{l, entry_front(f)});
+      return true;
+    }
+    return false;
+  };
+  for (size_t q = 0; q < seeds.size(); q++) {
+    const long long l = seeds[q];
+    S.t[l] = seedtt[q];
+    S.code[l] = (uint8_t)(CODE_NONE | CODE_SRC_BIT);
+    S.kL[l] = -EIK_INF;
+    S.kd[l] = 0;
+  }
+  double nm = EIK_INF;
+  for (size_t q = 0; q < seeds.size(); q++) {
+    const long long l = seeds[q];
+    int c[3];
+    S.coords(l, c);
+    if (seedtt[q] < EIK_INF) nm = std::fmin(nm, seedtt[q]);
+    for (int ax = 0; ax < ND; ax++)
+      for (int d = -2; d <= 2; d++) {
+        if (d == 0) continue;
+        int p[3] = {c[0], c[1], c[2]};
+        p[ax] += d;
+        if (p[ax] < 0 || p[ax] >= S.n[ax]) continue;
+        list(0, S.lin(p), seedtt[q], cur);
+      }
+  }
+  std::vector<int> parked_at(S.N, -1);
+  // parked nodes (mode 2): (front, node, round parked), smallest front first; an entry is
+  // live while the node is still parked from that round (a listing by a neighbour, or a
+  // later parking, supersedes it)
+  typedef std::tuple<double, long long, int> Parked;
+  std::priority_queue<Parked, std::vector<Parked>, std::greater<Parked>> park;
+  auto live = [&](const Parked& p) { return parked_at[std::get<1>(p)] == std::get<2>(p); };
+  long long entries = 0, unparked = 0;
+  int r = 0;
+  for (;; r++) {
+    // parked nodes whose front the threshold of this round can reach come back
+    double pmin = EIK_INF;
+    while (!park.empty() && !live(park.top())) park.pop();
+    if (!park.empty()) pmin = std::get<0>(park.top());
+    const double T = std::fmax(thr, std::fmin(nm, pmin) + S.delta);
+    while (!park.empty() && std::get<0>(park.top()) <= T) {
+      const Parked p = park.top();
+      park.pop();
+      if (!live(p)) continue;
+      parked_at[std::get<1>(p)] = -1;
+      if (list(r, std::get<1>(p), std::get<0>(p), cur)) unparked++;
+    }
+    if (cur.empty()) break;
+    thr = T;
+    entries += (long long)cur.size();
+    if (mode >= 1) std::shuffle(cur.begin(), cur.end(), rng);
+    next.clear();
+    nm_next = EIK_INF;
+    for (const Entry& e : cur) {
+      unsigned dirs = 0;
+      double front = EIK_INF;
+      int oc;
+      if (e.f > T && e.f < EIK_INF && !S.dirty[e.l]) {
+        front = e.f;
+        dirs = 1u << 12;
+        oc = V_STANDS;
+      } else {
+        dirs = visit<ND>(S, e.l, T, r, &front, &oc);
+      }
+      S.visits[oc]++;
+      bool kept = false;
+      for (int k = 0; k <= 12; k++) {
+        if (!((dirs >> k) & 1u)) continue;
+        const long long nl = dir_node(S, e.l, k);
+        if (mode == 2 && k == 12 && (oc == V_STANDS || oc == V_BOUND || oc == V_WAIT) && !S.dirty[nl] &&
+            S.stamp[nl] != r + 1) {
+          parked_at[nl] = r;  // waiting above the front: parked instead of listed again
+          park.push(Parked{entry_front(front), nl, r});
+          continue;
+        }
+        if (list(r + 1, nl, front, next)) {
+          kept = true;
+          parked_at[nl] = -1;
+        }
+      }
+      if (kept) nm_next = std::fmin(nm_next, front);
+    }
+    std::swap(cur, next);
+    nm = nm_next;
+  }
+  *rounds_out = r;
+  *entries_out = entries;
+  *unparked_out = unparked;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 3) {
+    std::fprintf(stderr, "usage: %s in.bin out.bin\n", argv[0]);
+    return 2;
+  }
+  FILE* f = std::fopen(argv[1], "rb");
+  if (!f) return 3;
+  int32_t hdr[4];
+  double hg[2];
+  int32_t mode;
+  uint64_t seed;
+  int64_t nseed;
+  if (std::fread(hdr, 4, 4, f) != 4 || std::fread(hg, 8, 2, f) != 2 || std::fread(&mode, 4, 1, f) != 1 ||
+      std::fread(&seed, 8, 1, f) != 1 || std::fread(&nseed, 8, 1, f) != 1)
+    return 4;
+  Solver S;
+  S.nd = hdr[0];
+  S.n[0] = hdr[1];
+  S.n[1] = hdr[2];
+  S.n[2] = hdr[3];
+  S.h = hg[0];
+  S.N = (long long)S.n[0] * S.n[1] * S.n[2];
+  S.slow.resize(S.N);
+  std::vector<long long> seeds(nseed);
+  std::vector<double> seedtt(nseed);
+  if (std::fread(S.slow.data(), 8, S.N, f) != (size_t)S.N || std::fread(seeds.data(), 8, nseed, f) != (size_t)nseed ||
+      std::fread(seedtt.data(), 8, nseed, f) != (size_t)nseed)
+    return 5;
+  std::fclose(f);
+  S.t.assign(S.N, EIK_INF);
+  S.tent.assign(S.N, EIK_INF);
+  S.kL.assign(S.N, 0.0);
+  S.code.assign(S.N, CODE_NONE);
+  S.kd.assign(S.N, 0);
+  S.dirty.assign(S.N, 1);
+  S.stamp.assign(S.N, -1);
+  double smin = EIK_INF;
+  for (double s : S.slow) smin = std::fmin(smin, s);
+  const double hmin = S.h;
+  S.delta = hg[1] * hmin * smin;
+  S.incmin = 0.999 * (2.0 / 3.0) * hmin * smin / std::sqrt((double)S.nd);
+  S.c1u = 1.0 / (S.h * S.h);
+  S.c2u = 9.0 / (4.0 * (S.h * S.h));
+  long long rounds = 0, entries = 0, unparked = 0;
+  if (S.nd == 3)
+    solve<3>(S, seeds, seedtt, mode, seed, &rounds, &entries, &unparked);
+  else
+    solve<2>(S, seeds, seedtt, mode, seed, &rounds, &entries, &unparked);
+  FILE* o = std::fopen(argv[2], "wb");
+  if (!o) return 6;
+  std::fwrite(S.t.data(), 8, S.N, o);
+  const int64_t st[11] = {rounds, entries, S.evals, S.visits[0], S.visits[1], S.visits[2],
+                          S.visits[3], S.visits[4], S.visits[5], S.visits[6], unparked};
+  std::fwrite(st, 8, 11, o);
+  std::fclose(o);
+  return 0;
+}
