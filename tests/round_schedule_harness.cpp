@@ -8,7 +8,9 @@
 // a round run in list order (mode 0), in a seeded random order (mode 1), or in a random order
 // with waiting nodes parked by front instead of listed again every round (mode 2: a node
 // whose front still stands is taken out of the lists and comes back in the first round whose
-// threshold reaches its front, unless a neighbour's change lists it earlier).
+// threshold reaches its front, unless a neighbour's change lists it earlier; modes 3-6: the
+// same with the parked nodes in buckets of 1, 1/4, 1/16 or 1/64 round width by front, a bucket
+// coming back whole once the threshold reaches its smallest front).
 //
 // Usage: round_schedule_harness in.bin out.bin
 //   in:  int32 nd, n0, n1, n2; double h, gate; int32 mode; uint64 seed; int64 nseed;
@@ -22,6 +24,7 @@
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <queue>
 #include <tuple>
 #include <random>
@@ -303,6 +306,11 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
   typedef std::tuple<double, long long, int> Parked;
   std::priority_queue<Parked, std::vector<Parked>, std::greater<Parked>> park;
   auto live = [&](const Parked& p) { return parked_at[std::get<1>(p)] == std::get<2>(p); };
+  // modes 3-6: parked nodes in buckets by front (1, 1/4, 1/16, 1/64 of the round width),
+  // each with its smallest front; a bucket comes back whole once the threshold reaches its
+  // smallest front (the form a device queue in memory would take)
+  std::map<long long, std::vector<Parked>> buckets;
+  std::map<long long, double> bucket_min;
   long long entries = 0, unparked = 0;
   int r = 0;
   for (;; r++) {
@@ -310,6 +318,15 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
     double pmin = EIK_INF;
     while (!park.empty() && !live(park.top())) park.pop();
     if (!park.empty()) pmin = std::get<0>(park.top());
+    while (!bucket_min.empty()) {  // buckets left with superseded entries only
+      const long long b = bucket_min.begin()->first;
+      bool any = false;
+      for (const Parked& p : buckets[b]) any = any || live(p);
+      if (any) break;
+      buckets.erase(b);
+      bucket_min.erase(b);
+    }
+    if (!bucket_min.empty()) pmin = bucket_min.begin()->second;
     const double T = std::fmax(thr, std::fmin(nm, pmin) + S.delta);
     while (!park.empty() && std::get<0>(park.top()) <= T) {
       const Parked p = park.top();
@@ -317,6 +334,16 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
       if (!live(p)) continue;
       parked_at[std::get<1>(p)] = -1;
       if (list(r, std::get<1>(p), std::get<0>(p), cur)) unparked++;
+    }
+    while (!bucket_min.empty() && bucket_min.begin()->second <= T) {
+      const long long b = bucket_min.begin()->first;
+      for (const Parked& p : buckets[b]) {
+        if (!live(p)) continue;
+        parked_at[std::get<1>(p)] = -1;
+        if (list(r, std::get<1>(p), std::get<0>(p), cur)) unparked++;
+      }
+      buckets.erase(b);
+      bucket_min.erase(b);
     }
     if (cur.empty()) break;
     thr = T;
@@ -340,10 +367,19 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
       for (int k = 0; k <= 12; k++) {
         if (!((dirs >> k) & 1u)) continue;
         const long long nl = dir_node(S, e.l, k);
-        if (mode == 2 && k == 12 && (oc == V_STANDS || oc == V_BOUND || oc == V_WAIT) && !S.dirty[nl] &&
+        if (mode >= 2 && k == 12 && (oc == V_STANDS || oc == V_BOUND || oc == V_WAIT) && !S.dirty[nl] &&
             S.stamp[nl] != r + 1) {
           parked_at[nl] = r;  // waiting above the front: parked instead of listed again
-          park.push(Parked{entry_front(front), nl, r});
+          const double pf = entry_front(front);
+          if (mode == 2) {
+            park.push(Parked{pf, nl, r});
+          } else {
+            const double bw = S.delta / (mode == 3 ? 1.0 : (double)(1 << (2 * (mode - 3))));
+            const long long b = (long long)std::floor(pf / bw);
+            buckets[b].push_back(Parked{pf, nl, r});
+            auto it = bucket_min.find(b);
+            if (it == bucket_min.end() || pf < it->second) bucket_min[b] = pf;
+          }
           continue;
         }
         if (list(r + 1, nl, front, next)) {

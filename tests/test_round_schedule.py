@@ -2,7 +2,8 @@
 node visit of node.cuh restated one visit at a time around the product's order rule, stencil.cuh
 compiled for the host), reaches the oracle's heap-FMM traveltimes bit for bit whatever the
 order of the visits within a round and whatever the round width, and also when nodes waiting
-above the front are parked by front instead of listed again every round. The kernels run the
+above the front are parked by front (exactly, or in buckets by front) instead of listed again
+every round. The kernels run the
 same visit with concurrent visits inside a round; these runs pin that the fixed point does not
 depend on the order in which a round's entries are taken, on all 16 reference cases and two
 seeded workloads, without a GPU."""
@@ -69,7 +70,7 @@ def _check(out, tt, stats):
 @pytest.mark.parametrize("case", RC.all_forward_cases(), ids=lambda c: c["name"])
 def test_reference_cases_any_order_any_width(harness, case):
     src = np.atleast_2d(case["coordsrc"])[0]
-    for gate, mode, seed in [(1.0, 0, 0), (0.5, 1, 1), (2.0, 1, 2), (8.0, 1, 3), (1.0, 2, 4)]:
+    for gate, mode, seed in [(1.0, 0, 0), (0.5, 1, 1), (2.0, 1, 2), (8.0, 1, 3), (1.0, 2, 4), (1.0, 5, 5)]:
         _check(*_emulate(harness, case["vel"], case["grd"], src, gate, mode, seed))
 
 
@@ -77,19 +78,21 @@ def test_reference_cases_any_order_any_width(harness, case):
 def test_seeded_workloads_any_order(harness, which):
     w = CF.cfg1() if which == "cfg1_300x220" else CF.cfg3(scale=0.125, nsrc=2, nrec_side=3)
     for s, src in enumerate(w.coordsrc[:2]):
-        for gate, mode, seed in [(1.0, 1, 10 + s), (4.0, 1, 20 + s), (1.0, 2, 30 + s)]:
+        for gate, mode, seed in [(1.0, 1, 10 + s), (4.0, 1, 20 + s), (1.0, 2, 30 + s), (1.0, 3, 40 + s)]:
             _check(*_emulate(harness, w.vel, w.grd, src, gate, mode, seed))
 
 
 def test_parking_waiting_nodes_saves_list_entries(harness):
     """Waiting nodes are most of the list entries at narrow round widths: parking them by
     front leaves the result unchanged and takes about a third fewer entries (300x220 at round
-    width 1)."""
+    width 1); buckets of 1/16 round width by front keep most of that."""
     w = CF.cfg1()
     src = w.coordsrc[0]
     out1, tt, listed = _emulate(harness, w.vel, w.grd, src, 1.0, 1, 5)
     out2, _, parked = _emulate(harness, w.vel, w.grd, src, 1.0, 2, 5)
-    _check(out1, tt, listed)
-    _check(out2, tt, parked)
-    assert parked["unparked"] > 0
+    out3, _, bucketed = _emulate(harness, w.vel, w.grd, src, 1.0, 5, 5)
+    for o, st in ((out1, listed), (out2, parked), (out3, bucketed)):
+        _check(o, tt, st)
+    assert parked["unparked"] > 0 and bucketed["unparked"] > 0
     assert parked["entries"] < 0.8 * listed["entries"], (parked["entries"], listed["entries"])
+    assert bucketed["entries"] < 0.8 * listed["entries"], (bucketed["entries"], listed["entries"])
