@@ -10,7 +10,9 @@
 // whose front still stands is taken out of the lists and comes back in the first round whose
 // threshold reaches its front, unless a neighbour's change lists it earlier; modes 3-6: the
 // same with the parked nodes in buckets of 1, 1/4, 1/16 or 1/64 round width by front, a bucket
-// coming back whole once the threshold reaches its smallest front).
+// coming back whole once the threshold reaches its smallest front). Mode 7 runs each round's
+// visits as concurrent visits may interleave at the extreme: all reads at the round's start,
+// then all writes, then all relist filters, each in a random order.
 //
 // Usage: round_schedule_harness in.bin out.bin
 //   in:  int32 nd, n0, n1, n2; double h, gate; int32 mode; uint64 seed; int64 nseed;
@@ -74,10 +76,28 @@ double entry_front(double f) {
 
 enum { V_STANDS, V_SOURCE, V_UNREACHED, V_BOUND, V_WAIT, V_SAME, V_CHANGED };
 
-// One visit of node l in round r under threshold T (node.cuh, process_node). Returns the
-// directions to list (bit 4*ax+j for j = -2,-1,+1,+2; bit 12 itself) and the outcome.
+// What a visit decides from what it reads (node.cuh, process_node): its outcome, the
+// direction bit of the node itself for the waiting outcomes, the front, and the writes to its
+// own node. evaluate() only reads; commit() writes; relist() is the filter that follows an
+// accepted change, reading the state as it is then.
+struct Visit {
+  int outcome = 0;
+  unsigned dirs = 0;
+  double front = EIK_INF;
+  bool clear_dirty = false;  // the visit reads its neighbours: its dirty flag is cleared first
+  bool set_tent = false;
+  double tent = EIK_INF;
+  bool set_code = false;
+  uint8_t code = 0;
+  bool changed = false;  // value or key accepted: t, code and key are written, then the filter
+  double nv = EIK_INF;
+  Key nk{}, kold{};
+  bool special = false;
+};
+
 template <int ND>
-unsigned visit(Solver& S, long long l, double T, int r, double* front, int* outcome) {
+Visit evaluate(const Solver& S, long long l, double T) {
+  Visit v;
   int c[3];
   S.coords(l, c);
   const uint8_t dirty0 = S.dirty[l];
@@ -85,18 +105,19 @@ unsigned visit(Solver& S, long long l, double T, int r, double* front, int* outc
   const uint8_t cb = S.code[l];
   const double told = S.t[l];
   if (!dirty0 && tv > T && tv < EIK_INF) {
-    *front = tv;
-    *outcome = V_STANDS;
-    return 1u << 12;
+    v.front = tv;
+    v.outcome = V_STANDS;
+    v.dirs = 1u << 12;
+    return v;
   }
   double Lold;
   int dold;
   S.key(l, told, cb, &Lold, &dold);
   if ((cb & CODE_SRC_BIT) && Lold == -EIK_INF) {
-    *outcome = V_SOURCE;
-    return 0;
+    v.outcome = V_SOURCE;
+    return v;
   }
-  S.dirty[l] = 0;
+  v.clear_dirty = true;
   long long l1[3][2], l2[3][2];
   double t1[3][2], t2[3][2];
   uint8_t cd1[3][2], cd2[3][2];
@@ -111,18 +132,21 @@ unsigned visit(Solver& S, long long l, double T, int r, double* front, int* outc
       pot = std::fmin(pot, t1[ax][s]);
     }
   if (!(pot < EIK_INF)) {
-    S.tent[l] = EIK_INF;
-    *outcome = V_UNREACHED;
-    return 0;
+    v.set_tent = true;
+    v.tent = EIK_INF;
+    v.outcome = V_UNREACHED;
+    return v;
   }
   const double slow = S.slow[l];
   const double hmin = S.h;
   const double lb = pot + 0.999 * (2.0 / 3.0) * hmin * slow * (ND == 3 ? 0.5773502691896258 : 0.7071067811865476);
   if (lb > T) {
-    S.tent[l] = lb;
-    *front = lb;
-    *outcome = V_BOUND;
-    return 1u << 12;
+    v.set_tent = true;
+    v.tent = lb;
+    v.front = lb;
+    v.outcome = V_BOUND;
+    v.dirs = 1u << 12;
+    return v;
   }
   bool plain = true;
   for (int ax = 0; ax < ND; ax++)
@@ -194,31 +218,56 @@ unsigned visit(Solver& S, long long l, double T, int r, double* front, int* outc
       }
     nv = prefix_rule<ND>(nb, cd, &nk, &neg);
   }
-  S.evals++;
   const uint8_t nc = pack_codes(cd, ND);
   const bool same_t = (nv == told) || (std::isinf(nv) && std::isinf(told));
   const bool tkchange = !(same_t && key_eq(nk, Key{Lold, dold, told}));
   const bool special = !(nk.L == nv && nk.d == 0);
   const uint8_t ncb = (uint8_t)(nc | (special ? CODE_SRC_BIT : 0));
-  S.tent[l] = nv;
+  v.set_tent = true;
+  v.tent = nv;
   if (!tkchange) {
-    if (ncb != cb) S.code[l] = ncb;
-    *outcome = V_SAME;
-    return 0;
+    v.set_code = ncb != cb;
+    v.code = ncb;
+    v.outcome = V_SAME;
+    return v;
   }
   if (nv > T) {
-    *front = nv;
-    *outcome = V_WAIT;
-    return 1u << 12;
+    v.front = nv;
+    v.outcome = V_WAIT;
+    v.dirs = 1u << 12;
+    return v;
   }
-  S.t[l] = nv;
-  S.code[l] = ncb;
-  if (special) {
-    S.kL[l] = nk.L;
-    S.kd[l] = (uint8_t)nk.d;
+  v.changed = true;
+  v.set_code = true;
+  v.code = ncb;
+  v.nv = nv;
+  v.nk = nk;
+  v.kold = Key{Lold, dold, told};
+  v.special = special;
+  v.front = nv + S.incmin;
+  v.outcome = V_CHANGED;
+  return v;
+}
+
+void commit(Solver& S, long long l, const Visit& v) {
+  if (v.set_tent) S.tent[l] = v.tent;
+  if (v.set_code) S.code[l] = v.code;
+  if (v.changed) {
+    S.t[l] = v.nv;
+    if (v.special) {
+      S.kL[l] = v.nk.L;
+      S.kd[l] = (uint8_t)v.nk.d;
+    }
   }
-  // relist filter
-  const Key kold = Key{Lold, dold, told};
+}
+
+// The relist filter after an accepted change of node l in round r: the nodes whose stencil
+// reads l, except those whose key is at most both the old and the new key of l and that are
+// in no list of this round or the next.
+template <int ND>
+unsigned relist(Solver& S, long long l, const Visit& v, int r) {
+  int c[3];
+  S.coords(l, c);
   unsigned dirs = 0;
   for (int ax = 0; ax < ND; ax++) {
     long long lj[4];
@@ -239,14 +288,12 @@ unsigned visit(Solver& S, long long l, double T, int r, double* front, int* outc
         int dj;
         S.key(lj[j], tj[j], S.code[lj[j]], &Lj, &dj);
         const Key kj = Key{Lj, dj, tj[j]};
-        if (key_le(kj, kold) && key_le(kj, nk)) continue;
+        if (key_le(kj, v.kold) && key_le(kj, v.nk)) continue;
       }
       S.dirty[lj[j]] = 1;
       dirs |= 1u << (4 * ax + j);
     }
   }
-  *front = nv + S.incmin;
-  *outcome = V_CHANGED;
   return dirs;
 }
 
@@ -346,29 +393,60 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
       bucket_min.erase(b);
     }
     if (cur.empty()) break;
+    if (r >= (1 << 20)) break;  // not settling: reported as 2^20 rounds
     thr = T;
     entries += (long long)cur.size();
     if (mode >= 1) std::shuffle(cur.begin(), cur.end(), rng);
     next.clear();
     nm_next = EIK_INF;
-    for (const Entry& e : cur) {
-      unsigned dirs = 0;
-      double front = EIK_INF;
-      int oc;
+    // the visits of the round: one after the other (modes 0-6), or all reads first, then all
+    // writes, then all filters, each in a random order (mode 7: the extreme interleaving of
+    // concurrent visits, every visit seeing the state of the round's start)
+    std::vector<Visit> vs(cur.size());
+    auto take = [&](size_t i) {
+      const Entry& e = cur[i];
       if (e.f > T && e.f < EIK_INF && !S.dirty[e.l]) {
-        front = e.f;
-        dirs = 1u << 12;
-        oc = V_STANDS;
+        vs[i] = Visit();
+        vs[i].front = e.f;
+        vs[i].dirs = 1u << 12;
+        vs[i].outcome = V_STANDS;
       } else {
-        dirs = visit<ND>(S, e.l, T, r, &front, &oc);
+        vs[i] = evaluate<ND>(S, e.l, T);
       }
+    };
+    if (mode != 7) {
+      for (size_t i = 0; i < cur.size(); i++) {
+        take(i);
+        const long long l = cur[i].l;
+        if (vs[i].clear_dirty) S.dirty[l] = 0;
+        commit(S, l, vs[i]);
+        if (vs[i].changed) vs[i].dirs |= relist<ND>(S, l, vs[i], r);
+      }
+    } else {
+      for (size_t i = 0; i < cur.size(); i++) take(i);
+      for (size_t i = 0; i < cur.size(); i++)
+        if (vs[i].clear_dirty) S.dirty[cur[i].l] = 0;
+      std::vector<size_t> ord(cur.size());
+      for (size_t i = 0; i < ord.size(); i++) ord[i] = i;
+      std::shuffle(ord.begin(), ord.end(), rng);
+      for (size_t i : ord) commit(S, cur[i].l, vs[i]);
+      std::shuffle(ord.begin(), ord.end(), rng);
+      for (size_t i : ord)
+        if (vs[i].changed) vs[i].dirs |= relist<ND>(S, cur[i].l, vs[i], r);
+    }
+    for (size_t i = 0; i < cur.size(); i++) {
+      const Entry& e = cur[i];
+      const unsigned dirs = vs[i].dirs;
+      const double front = vs[i].front;
+      const int oc = vs[i].outcome;
+      if (oc >= V_WAIT) S.evals++;
       S.visits[oc]++;
       bool kept = false;
       for (int k = 0; k <= 12; k++) {
         if (!((dirs >> k) & 1u)) continue;
         const long long nl = dir_node(S, e.l, k);
-        if (mode >= 2 && k == 12 && (oc == V_STANDS || oc == V_BOUND || oc == V_WAIT) && !S.dirty[nl] &&
-            S.stamp[nl] != r + 1) {
+        if (mode >= 2 && mode <= 6 && k == 12 && (oc == V_STANDS || oc == V_BOUND || oc == V_WAIT) &&
+            !S.dirty[nl] && S.stamp[nl] != r + 1) {
           parked_at[nl] = r;  // waiting above the front: parked instead of listed again
           const double pf = entry_front(front);
           if (mode == 2) {

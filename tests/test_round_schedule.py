@@ -1,12 +1,12 @@
 """The forward round solver's schedule, emulated on the host (round_schedule_harness.cpp: the
-node visit of node.cuh restated one visit at a time around the product's order rule, stencil.cuh
-compiled for the host), reaches the oracle's heap-FMM traveltimes bit for bit whatever the
-order of the visits within a round and whatever the round width, and also when nodes waiting
-above the front are parked by front (exactly, or in buckets by front) instead of listed again
-every round. The kernels run the
-same visit with concurrent visits inside a round; these runs pin that the fixed point does not
-depend on the order in which a round's entries are taken, on all 16 reference cases and two
-seeded workloads, without a GPU."""
+node visit of node.cuh restated around the product's order rule, stencil.cuh compiled for the
+host), reaches the oracle's heap-FMM traveltimes bit for bit whatever the order of the visits
+within a round and whatever the round width: visits one after the other in list or random
+order, visits interleaved at the extreme concurrent visits allow (all of a round's reads, then
+all its writes, then all its relist filters), and nodes waiting above the front parked by front
+(exactly, or in buckets by front) instead of listed again every round. The kernels run the
+same visit with concurrent visits inside a round; these runs pin, on all 16 reference cases and
+two seeded workloads and without a GPU, that the fixed point does not depend on the order."""
 import os
 import shutil
 import struct
@@ -70,7 +70,8 @@ def _check(out, tt, stats):
 @pytest.mark.parametrize("case", RC.all_forward_cases(), ids=lambda c: c["name"])
 def test_reference_cases_any_order_any_width(harness, case):
     src = np.atleast_2d(case["coordsrc"])[0]
-    for gate, mode, seed in [(1.0, 0, 0), (0.5, 1, 1), (2.0, 1, 2), (8.0, 1, 3), (1.0, 2, 4), (1.0, 5, 5)]:
+    for gate, mode, seed in [(1.0, 0, 0), (0.5, 1, 1), (2.0, 1, 2), (8.0, 1, 3), (1.0, 2, 4), (1.0, 5, 5),
+                             (1.0, 7, 6), (4.0, 7, 7)]:
         _check(*_emulate(harness, case["vel"], case["grd"], src, gate, mode, seed))
 
 
@@ -78,7 +79,8 @@ def test_reference_cases_any_order_any_width(harness, case):
 def test_seeded_workloads_any_order(harness, which):
     w = CF.cfg1() if which == "cfg1_300x220" else CF.cfg3(scale=0.125, nsrc=2, nrec_side=3)
     for s, src in enumerate(w.coordsrc[:2]):
-        for gate, mode, seed in [(1.0, 1, 10 + s), (4.0, 1, 20 + s), (1.0, 2, 30 + s), (1.0, 3, 40 + s)]:
+        for gate, mode, seed in [(1.0, 1, 10 + s), (4.0, 1, 20 + s), (1.0, 2, 30 + s), (1.0, 3, 40 + s),
+                                 (1.0, 7, 50 + s)]:
             _check(*_emulate(harness, w.vel, w.grd, src, gate, mode, seed))
 
 
