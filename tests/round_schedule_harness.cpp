@@ -12,7 +12,13 @@
 // same with the parked nodes in buckets of 1, 1/4, 1/16 or 1/64 round width by front, a bucket
 // coming back whole once the threshold reaches its smallest front). Mode 7 runs each round's
 // visits as concurrent visits may interleave at the extreme: all reads at the round's start,
-// then all writes, then all relist filters, each in a random order.
+// then all writes, then all relist filters, each in a random order. Mode 8 runs them one
+// after the other in a random order, each read of a neighbour written earlier in the round
+// returning, at random, its value of the round's start or its current one (a traveltime and
+// the code beside it may disagree, as unordered loads of concurrent visits may; modes 9-11 tie
+// some of a neighbour's fields to one moment, see Solver::agree); such a read
+// places the visit before that neighbour's change, so the neighbour's relist filter leaves the
+// visited node's dirty flag set.
 //
 // Usage: round_schedule_harness in.bin out.bin
 //   in:  int32 nd, n0, n1, n2; double h, gate; int32 mode; uint64 seed; int64 nseed;
@@ -20,7 +26,7 @@
 //        nseed doubles traveltimes of the fixed source points.
 //   out: N doubles traveltime; int64 rounds, list entries, rule evaluations, visits by
 //        outcome (7: stands, source, unreached, bound, wait, same, changed), parked nodes
-//        taken back.
+//        taken back, nodes whose rule would still change their value or key at the end.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -48,6 +54,57 @@ struct Solver {
   std::vector<int> stamp;
   double delta, incmin, c1u, c2u;
   long long evals = 0, visits[7] = {0, 0, 0, 0, 0, 0, 0};
+  // mode 8: a neighbour written earlier in the round is read at its value of the round's
+  // start or at its current one, each read on its own (old_* hold the start values)
+  bool stale = false;
+  int round = -1;
+  std::vector<int> wround;
+  std::vector<double> old_t, old_kL;
+  std::vector<uint8_t> old_code, old_kd;
+  mutable std::mt19937_64 coin{12345};
+  mutable bool saw_stale = false;
+  // how the reads of one neighbour within a visit agree (modes 8-11): 0 each read on its own;
+  // 1 traveltime, code and key level from the same moment; 2 code and key level together,
+  // the traveltime on its own; 3 traveltime and code together, the key level on its own
+  int agree = 0;
+  mutable std::vector<std::pair<long long, unsigned>> picks;  // this visit's choices per node
+  bool old_of(long long x, int field) const {  // field 0: t, 1: code, 2: key level
+    if (!(stale && wround[x] == round)) return false;
+    const int group = agree == 0 ? field : (agree == 1 ? 0 : (agree == 2 ? (field == 0 ? 0 : 1) : (field == 2 ? 1 : 0)));
+    unsigned have = 0, bits = 0;
+    for (auto& pr : picks)
+      if (pr.first == x) {
+        have = pr.second & 3u;
+        bits = pr.second >> 2;
+      }
+    bool o;
+    if (agree != 0 && ((have >> group) & 1u)) {
+      o = (bits >> group) & 1u;
+    } else {
+      o = coin() & 1u;
+      bool found = false;
+      for (auto& pr : picks)
+        if (pr.first == x) {
+          pr.second |= (1u << group) | ((o ? 1u : 0u) << (2 + group));
+          found = true;
+        }
+      if (!found) picks.push_back({x, (1u << group) | ((o ? 1u : 0u) << (2 + group))});
+    }
+    saw_stale = saw_stale || o;
+    return o;
+  }
+  double rt(long long x) const { return old_of(x, 0) ? old_t[x] : t[x]; }
+  uint8_t rc(long long x) const { return old_of(x, 1) ? old_code[x] : code[x]; }
+  void rkey(long long x, double tv, uint8_t cb, double* L, int* d) const {
+    if (cb & CODE_SRC_BIT) {
+      const bool o = old_of(x, 2);
+      *L = o ? old_kL[x] : kL[x];
+      *d = o ? old_kd[x] : kd[x];
+    } else {
+      *L = tv;
+      *d = 0;
+    }
+  }
 
   long long lin(const int* c) const { return c[0] + (long long)n[0] * (c[1] + (long long)n[1] * c[2]); }
   void coords(long long l, int* c) const {
@@ -128,7 +185,7 @@ Visit evaluate(const Solver& S, long long l, double T) {
       int p[3] = {c[0], c[1], c[2]};
       p[ax] += sh;
       l1[ax][s] = (p[ax] < 0 || p[ax] >= S.n[ax]) ? -1 : S.lin(p);
-      t1[ax][s] = l1[ax][s] >= 0 ? S.t[l1[ax][s]] : EIK_INF;
+      t1[ax][s] = l1[ax][s] >= 0 ? S.rt(l1[ax][s]) : EIK_INF;
       pot = std::fmin(pot, t1[ax][s]);
     }
   if (!(pot < EIK_INF)) {
@@ -156,7 +213,7 @@ Visit evaluate(const Solver& S, long long l, double T) {
       cd1[ax][s] = cd2[ax][s] = 0;
       t2[ax][s] = EIK_INF;
       if (l1[ax][s] < 0) continue;
-      cd1[ax][s] = S.code[l1[ax][s]];
+      cd1[ax][s] = S.rc(l1[ax][s]);
       int p[3] = {c[0], c[1], c[2]};
       p[ax] += sh;
       bool ok = true;  // isonbord on the first neighbour
@@ -165,8 +222,8 @@ Visit evaluate(const Solver& S, long long l, double T) {
       if (ok) {
         p[ax] += sh;
         l2[ax][s] = S.lin(p);
-        t2[ax][s] = S.t[l2[ax][s]];
-        cd2[ax][s] = S.code[l2[ax][s]];
+        t2[ax][s] = S.rt(l2[ax][s]);
+        cd2[ax][s] = S.rc(l2[ax][s]);
       }
       if ((cd1[ax][s] | cd2[ax][s]) & CODE_SRC_BIT) plain = false;
     }
@@ -209,10 +266,10 @@ Visit evaluate(const Solver& S, long long l, double T) {
         if (l1[ax][s] < 0) continue;
         double L;
         int d;
-        S.key(l1[ax][s], t1[ax][s], cd1[ax][s], &L, &d);
+        S.rkey(l1[ax][s], t1[ax][s], cd1[ax][s], &L, &d);
         nb_put1(nb, ax, s, t1[ax][s], L, d);
         if (l2[ax][s] >= 0) {
-          S.key(l2[ax][s], t2[ax][s], cd2[ax][s], &L, &d);
+          S.rkey(l2[ax][s], t2[ax][s], cd2[ax][s], &L, &d);
           nb_put2(nb, ax, s, t2[ax][s], L, d);
         }
       }
@@ -250,6 +307,13 @@ Visit evaluate(const Solver& S, long long l, double T) {
 }
 
 void commit(Solver& S, long long l, const Visit& v) {
+  if (S.stale && S.wround[l] != S.round && v.changed) {
+    S.wround[l] = S.round;  // first write of the round: keep the start values
+    S.old_t[l] = S.t[l];
+    S.old_code[l] = S.code[l];
+    S.old_kL[l] = S.kL[l];
+    S.old_kd[l] = S.kd[l];
+  }
   if (v.set_tent) S.tent[l] = v.tent;
   if (v.set_code) S.code[l] = v.code;
   if (v.changed) {
@@ -314,6 +378,16 @@ template <int ND>
 void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<double>& seedtt, int mode,
            unsigned long long seed, long long* rounds_out, long long* entries_out, long long* unparked_out) {
   std::mt19937_64 rng(seed);
+  if (mode >= 8 && mode <= 11) {
+    S.stale = true;
+    S.agree = mode - 8;
+    S.coin.seed(seed ^ 0x9e3779b97f4a7c15ull);
+    S.wround.assign(S.N, -1);
+    S.old_t.assign(S.N, EIK_INF);
+    S.old_kL.assign(S.N, 0.0);
+    S.old_code.assign(S.N, CODE_NONE);
+    S.old_kd.assign(S.N, 0);
+  }
   std::vector<Entry> cur, next;
   double nm_next = EIK_INF, thr = -EIK_INF;
   auto list = [&](int r, long long l, double f, std::vector<Entry>& L) {
@@ -395,6 +469,7 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
     if (cur.empty()) break;
     if (r >= (1 << 20)) break;  // not settling: reported as 2^20 rounds
     thr = T;
+    S.round = r;
     entries += (long long)cur.size();
     if (mode >= 1) std::shuffle(cur.begin(), cur.end(), rng);
     next.clear();
@@ -416,9 +491,15 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
     };
     if (mode != 7) {
       for (size_t i = 0; i < cur.size(); i++) {
+        S.saw_stale = false;
+        S.picks.clear();
         take(i);
         const long long l = cur[i].l;
         if (vs[i].clear_dirty) S.dirty[l] = 0;
+        // a read of a neighbour's value from before its change this round means that, in
+        // real time, the read preceded that change, whose relist filter then ran after this
+        // visit had cleared its flag: the flag that filter set stands
+        if (S.saw_stale) S.dirty[l] = 1;
         commit(S, l, vs[i]);
         if (vs[i].changed) vs[i].dirs |= relist<ND>(S, l, vs[i], r);
       }
@@ -525,12 +606,21 @@ int main(int argc, char** argv) {
     solve<3>(S, seeds, seedtt, mode, seed, &rounds, &entries, &unparked);
   else
     solve<2>(S, seeds, seedtt, mode, seed, &rounds, &entries, &unparked);
+  // nodes whose order rule, evaluated on the final state with no threshold, would still change
+  // their value or key (0 for a fixed point)
+  S.stale = false;
+  long long unsettled = 0;
+  for (long long l = 0; l < S.N; l++) {
+    S.dirty[l] = 1;
+    const Visit v = S.nd == 3 ? evaluate<3>(S, l, EIK_INF) : evaluate<2>(S, l, EIK_INF);
+    if (v.changed) unsettled++;
+  }
   FILE* o = std::fopen(argv[2], "wb");
   if (!o) return 6;
   std::fwrite(S.t.data(), 8, S.N, o);
-  const int64_t st[11] = {rounds, entries, S.evals, S.visits[0], S.visits[1], S.visits[2],
-                          S.visits[3], S.visits[4], S.visits[5], S.visits[6], unparked};
-  std::fwrite(st, 8, 11, o);
+  const int64_t st[12] = {rounds, entries, S.evals, S.visits[0], S.visits[1], S.visits[2],
+                          S.visits[3], S.visits[4], S.visits[5], S.visits[6], unparked, unsettled};
+  std::fwrite(st, 8, 12, o);
   std::fclose(o);
   return 0;
 }

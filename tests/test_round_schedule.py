@@ -3,8 +3,10 @@ node visit of node.cuh restated around the product's order rule, stencil.cuh com
 host), reaches the oracle's heap-FMM traveltimes bit for bit whatever the order of the visits
 within a round and whatever the round width: visits one after the other in list or random
 order, visits interleaved at the extreme concurrent visits allow (all of a round's reads, then
-all its writes, then all its relist filters), and nodes waiting above the front parked by front
-(exactly, or in buckets by front) instead of listed again every round. The kernels run the
+all its writes, then all its relist filters), visits that read a neighbour changed earlier in
+the round at its old or its new state (with its traveltime, code and key level from one moment,
+or any two of them), and nodes waiting above the front parked by front (exactly, or in buckets
+by front) instead of listed again every round. The kernels run the
 same visit with concurrent visits inside a round; these runs pin, on all 16 reference cases and
 two seeded workloads and without a GPU, that the fixed point does not depend on the order."""
 import os
@@ -71,7 +73,7 @@ def _check(out, tt, stats):
 def test_reference_cases_any_order_any_width(harness, case):
     src = np.atleast_2d(case["coordsrc"])[0]
     for gate, mode, seed in [(1.0, 0, 0), (0.5, 1, 1), (2.0, 1, 2), (8.0, 1, 3), (1.0, 2, 4), (1.0, 5, 5),
-                             (1.0, 7, 6), (4.0, 7, 7)]:
+                             (1.0, 7, 6), (4.0, 7, 7), (2.0, 9, 8), (2.0, 10, 9), (2.0, 11, 10)]:
         _check(*_emulate(harness, case["vel"], case["grd"], src, gate, mode, seed))
 
 
