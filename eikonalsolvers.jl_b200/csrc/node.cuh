@@ -64,9 +64,14 @@ __device__ __forceinline__ void flush_visits(const unsigned long long* w, unsign
 }
 
 // ------------------------------------------------------------------ node solve --
-// Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise.
+// Key of node l of problem P: (L, d) of a special node, (t, 0) otherwise. A special key counts
+// only beside a reached traveltime. Every special node has one (a source point's or an
+// accepted value), so this changes nothing a consistent read sees; but a visit's loads of a
+// neighbour changed in the same round are unordered, and one that sees the new code beside
+// the old, unreached traveltime must not take a key level that belongs to neither (it made
+// NaN traveltimes and a wrong fixed point in a host emulation of such reads).
 __device__ __forceinline__ void node_key(const CoarseProblem& P, long long l, double t, uint8_t cb, double* L, int* d) {
-  if (cb & CODE_SRC_BIT) {
+  if ((cb & CODE_SRC_BIT) && t < EIK_INF) {
     *L = __ldcg(P.kL + l);
     *d = __ldcg(P.kd + l);
   } else {

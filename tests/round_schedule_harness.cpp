@@ -96,7 +96,7 @@ struct Solver {
   double rt(long long x) const { return old_of(x, 0) ? old_t[x] : t[x]; }
   uint8_t rc(long long x) const { return old_of(x, 1) ? old_code[x] : code[x]; }
   void rkey(long long x, double tv, uint8_t cb, double* L, int* d) const {
-    if (cb & CODE_SRC_BIT) {
+    if ((cb & CODE_SRC_BIT) && tv < EIK_INF) {
       const bool o = old_of(x, 2);
       *L = o ? old_kL[x] : kL[x];
       *d = o ? old_kd[x] : kd[x];
@@ -112,8 +112,9 @@ struct Solver {
     c[1] = (int)((l / n[0]) % n[1]);
     c[2] = (int)(l / ((long long)n[0] * n[1]));
   }
+  // node_key of node.cuh: a special key counts only beside a reached traveltime
   void key(long long l, double tv, uint8_t cb, double* L, int* d) const {
-    if (cb & CODE_SRC_BIT) {
+    if ((cb & CODE_SRC_BIT) && tv < EIK_INF) {
       *L = kL[l];
       *d = kd[l];
     } else {
@@ -384,7 +385,7 @@ void solve(Solver& S, const std::vector<long long>& seeds, const std::vector<dou
     S.coin.seed(seed ^ 0x9e3779b97f4a7c15ull);
     S.wround.assign(S.N, -1);
     S.old_t.assign(S.N, EIK_INF);
-    S.old_kL.assign(S.N, 0.0);
+    S.old_kL.assign(S.N, -EIK_INF);
     S.old_code.assign(S.N, CODE_NONE);
     S.old_kd.assign(S.N, 0);
   }
@@ -589,7 +590,7 @@ int main(int argc, char** argv) {
   std::fclose(f);
   S.t.assign(S.N, EIK_INF);
   S.tent.assign(S.N, EIK_INF);
-  S.kL.assign(S.N, 0.0);
+  S.kL.assign(S.N, -EIK_INF);  // never read unless written: any value will do, this one is the worst
   S.code.assign(S.N, CODE_NONE);
   S.kd.assign(S.N, 0);
   S.dirty.assign(S.N, 1);

@@ -4,9 +4,12 @@ host), reaches the oracle's heap-FMM traveltimes bit for bit whatever the order 
 within a round and whatever the round width: visits one after the other in list or random
 order, visits interleaved at the extreme concurrent visits allow (all of a round's reads, then
 all its writes, then all its relist filters), visits that read a neighbour changed earlier in
-the round at its old or its new state (with its traveltime, code and key level from one moment,
-or any two of them), and nodes waiting above the front parked by front (exactly, or in buckets
-by front) instead of listed again every round. The kernels run the
+the round at its old or its new state (its traveltime, code and key level each from its own
+moment, as unordered loads may see them, or tied together), and nodes waiting above the front
+parked by front (exactly, or in buckets by front) instead of listed again every round. Seeds 21
+and 37 of the independent-read mode are the orders in which 3Dconst2 and 3Dconst3 reached NaN
+traveltimes and a wrong fixed point before node_key ignored a special key beside an unreached
+traveltime. The kernels run the
 same visit with concurrent visits inside a round; these runs pin, on all 16 reference cases and
 two seeded workloads and without a GPU, that the fixed point does not depend on the order."""
 import os
@@ -73,7 +76,8 @@ def _check(out, tt, stats):
 def test_reference_cases_any_order_any_width(harness, case):
     src = np.atleast_2d(case["coordsrc"])[0]
     for gate, mode, seed in [(1.0, 0, 0), (0.5, 1, 1), (2.0, 1, 2), (8.0, 1, 3), (1.0, 2, 4), (1.0, 5, 5),
-                             (1.0, 7, 6), (4.0, 7, 7), (2.0, 9, 8), (2.0, 10, 9), (2.0, 11, 10)]:
+                             (1.0, 7, 6), (4.0, 7, 7), (2.0, 8, 11), (2.0, 8, 21), (2.0, 8, 37), (2.0, 9, 8),
+                             (2.0, 10, 9), (2.0, 11, 10)]:
         _check(*_emulate(harness, case["vel"], case["grd"], src, gate, mode, seed))
 
 
@@ -82,7 +86,7 @@ def test_seeded_workloads_any_order(harness, which):
     w = CF.cfg1() if which == "cfg1_300x220" else CF.cfg3(scale=0.125, nsrc=2, nrec_side=3)
     for s, src in enumerate(w.coordsrc[:2]):
         for gate, mode, seed in [(1.0, 1, 10 + s), (4.0, 1, 20 + s), (1.0, 2, 30 + s), (1.0, 3, 40 + s),
-                                 (1.0, 7, 50 + s)]:
+                                 (1.0, 7, 50 + s), (2.0, 8, 60 + s)]:
             _check(*_emulate(harness, w.vel, w.grd, src, gate, mode, seed))
 
 
