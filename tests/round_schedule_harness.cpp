@@ -26,7 +26,8 @@
 //        nseed doubles traveltimes of the fixed source points.
 //   out: N doubles traveltime; int64 rounds, list entries, rule evaluations, visits by
 //        outcome (7: stands, source, unreached, bound, wait, same, changed), parked nodes
-//        taken back, nodes whose rule would still change their value or key at the end.
+//        taken back, nodes whose rule would still change their value or key at the end,
+//        special nodes (code bit 7) left with an unreached traveltime.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -610,8 +611,9 @@ int main(int argc, char** argv) {
   // nodes whose order rule, evaluated on the final state with no threshold, would still change
   // their value or key (0 for a fixed point)
   S.stale = false;
-  long long unsettled = 0;
+  long long unsettled = 0, special_unreached = 0;
   for (long long l = 0; l < S.N; l++) {
+    if ((S.code[l] & CODE_SRC_BIT) && !(S.t[l] < EIK_INF)) special_unreached++;
     S.dirty[l] = 1;
     const Visit v = S.nd == 3 ? evaluate<3>(S, l, EIK_INF) : evaluate<2>(S, l, EIK_INF);
     if (v.changed) unsettled++;
@@ -619,9 +621,10 @@ int main(int argc, char** argv) {
   FILE* o = std::fopen(argv[2], "wb");
   if (!o) return 6;
   std::fwrite(S.t.data(), 8, S.N, o);
-  const int64_t st[12] = {rounds, entries, S.evals, S.visits[0], S.visits[1], S.visits[2],
-                          S.visits[3], S.visits[4], S.visits[5], S.visits[6], unparked, unsettled};
-  std::fwrite(st, 8, 12, o);
+  const int64_t st[13] = {rounds,      entries,     S.evals,     S.visits[0], S.visits[1],
+                          S.visits[2], S.visits[3], S.visits[4], S.visits[5], S.visits[6],
+                          unparked,    unsettled,   special_unreached};
+  std::fwrite(st, 8, 13, o);
   std::fclose(o);
   return 0;
 }

@@ -61,13 +61,16 @@ def _emulate(harness, vel, grd, src, gate, mode, seed):
     out = np.fromfile(fout, dtype=np.float64, count=tt.size)
     st = np.fromfile(fout, dtype=np.int64, offset=8 * tt.size)
     stats = dict(rounds=int(st[0]), entries=int(st[1]), evals=int(st[2]), visits=[int(x) for x in st[3:10]],
-                 unparked=int(st[10]))
+                 unparked=int(st[10]), unsettled=int(st[11]), special_unreached=int(st[12]))
     return out, tt, stats
 
 
 def _check(out, tt, stats):
     ndiff = int((out != tt).sum())
     assert ndiff == 0, f"{ndiff} nodes differ from the oracle"
+    assert stats["rounds"] < 1 << 20 and stats["unsettled"] == 0
+    # every special key sits beside a reached traveltime (what lets node_key ignore the others)
+    assert stats["special_unreached"] == 0
     assert sum(stats["visits"]) == stats["entries"]
     assert sum(stats["visits"][4:7]) == stats["evals"]
 
