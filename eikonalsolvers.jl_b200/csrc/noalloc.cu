@@ -12,9 +12,9 @@
 // last call's contents. Two calls whose work overlaps on the GPU (different streams, or
 // different host threads) race on it and give wrong results: serialise them.
 // The first call on each device does a one-time set-up (it looks up the array's device
-// address with cudaGetSymbolAddress); make that first call before any stream capture.
-// Every call copies the receiver offsets from host memory, reads its error word back to the
-// host and synchronises its stream: it blocks the calling thread until the misfit is written.
+// address with cudaGetSymbolAddress). Every call copies the receiver offsets from host
+// memory, reads its error word back to the host and synchronises its stream: it blocks the
+// calling thread until the misfit is written, and cannot run inside a stream capture.
 #include <mutex>
 
 #include "../../include/eikcuda.h"

@@ -269,11 +269,10 @@ int eik_traveltime_rays(eik_ctx* ctx, eik_model_id model, int64_t nsrc, const do
  * must not change the device's memory map). Its scratch is a fixed ~1 MB array in the
  * library, so nsrc is limited to 65536 (larger calls fail with EIK_ERR_OUT_OF_BUDGET).
  * All calls on a device share that array: calls that overlap on the GPU race, so
- * serialise them. The first call on each device looks up the array's address; make that
- * first call before any stream capture. Every call runs on `stream` (a cudaStream_t; NULL =
- * legacy default stream), copies rec_off from the host, reads its error word back into host
- * memory and synchronises `stream` before it returns: it blocks the calling host thread
- * until the result is written. */
+ * serialise them. Every call runs on `stream` (a cudaStream_t; NULL = legacy default
+ * stream), copies rec_off from the host, reads its error word back into host memory and
+ * synchronises `stream` before it returns: it blocks the calling host thread until the
+ * result is written, and no call can run while its stream is being captured into a graph. */
 int eik_ttimemisfit_noalloc(const eik_grid* grd, int64_t nsrc, const double* ttgrids_dev,
                             const int64_t* rec_off, const double* rec_dev, const double* pickobs_dev,
                             const double* stdobs_dev, double* misfit_dev, void* stream);
