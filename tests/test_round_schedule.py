@@ -11,7 +11,7 @@ and 37 of the independent-read mode are the orders in which 3Dconst2 and 3Dconst
 traveltimes and a wrong fixed point before node_key ignored a special key beside an unreached
 traveltime. The kernels run the
 same visit with concurrent visits inside a round; these runs pin, on all 16 reference cases and
-two seeded workloads and without a GPU, that the fixed point does not depend on the order."""
+three seeded workloads and without a GPU, that the fixed point does not depend on the order."""
 import os
 import shutil
 import struct
@@ -84,9 +84,16 @@ def test_reference_cases_any_order_any_width(harness, case):
         _check(*_emulate(harness, case["vel"], case["grd"], src, gate, mode, seed))
 
 
-@pytest.mark.parametrize("which", ["cfg1_300x220", "cfg3_32cubed"])
+_WORKLOADS = {
+    "cfg1_300x220": lambda: CF.cfg1(),
+    "cfg3_32cubed": lambda: CF.cfg3(scale=0.125, nsrc=2, nrec_side=3),
+    "cfg2_128x80_random_field": lambda: CF.cfg2(scale=0.125, nsrc=2),
+}
+
+
+@pytest.mark.parametrize("which", sorted(_WORKLOADS))
 def test_seeded_workloads_any_order(harness, which):
-    w = CF.cfg1() if which == "cfg1_300x220" else CF.cfg3(scale=0.125, nsrc=2, nrec_side=3)
+    w = _WORKLOADS[which]()
     for s, src in enumerate(w.coordsrc[:2]):
         for gate, mode, seed in [(1.0, 1, 10 + s), (4.0, 1, 20 + s), (1.0, 2, 30 + s), (1.0, 3, 40 + s),
                                  (1.0, 7, 50 + s), (2.0, 8, 60 + s)]:
